@@ -1,0 +1,63 @@
+"""Builds libabd_b200.so in-tree with nvcc for sm_100a.
+
+Each .cu under colb_b200/csrc is compiled to an object in parallel and the
+objects are linked into one shared library next to this file (the CUDA
+runtime is linked statically, so the library only needs the driver).
+"""
+import concurrent.futures as cf
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libabd_b200.so")
+BUILD = os.path.join(HERE, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xptxas", "-warn-spills"] + ARCH
+
+
+def _compile(src, extra):
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    deps = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(HERE, "..", "include", "abd_b200.h"), src]
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
+        return obj, ""
+    cmd = [NVCC] + FLAGS + extra + ["-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return obj, r.stderr
+
+
+def _sources():
+    return (glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+            [os.path.join(HERE, "..", "include", "abd_b200.h")])
+
+
+def up_to_date():
+    return os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(s) for s in _sources())
+
+
+def build(verbose=False, extra=()):
+    if up_to_date() and not extra:
+        return OUT
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        res = list(ex.map(lambda s: _compile(s, list(extra)), srcs))
+    objs = [o for o, _ in res]
+    if verbose:
+        for _, err in res:
+            if err.strip():
+                print(err)
+    if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart_static"]
+        subprocess.check_call(cmd)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

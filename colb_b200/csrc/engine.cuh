@@ -1,0 +1,193 @@
+// engine.cuh — device state of one ABD handle and the launch helpers.
+//
+// HBM layout (all scenes of a batch concatenated, body-major):
+//   st      [nb][48]  f64  BDFAffine (the reference's layout)
+//   xbar    [nv][3]   f64  rest positions in the body frame
+//   x       [nv][3]   f64  current positions of the nxt state
+//   xf      [nv]      f32x4 float copy used by the float32 EE predicate
+//   edges   [ne]      i32x2, tris [nt][3] i32, vbody [nv] i32, bscene [nb] i32
+//   g, du   [nb][12]  f64  gradient / Newton increment, DoF order [c q0 q1 q2]
+//   blocks  [nnzb][144]  f64 or f32  12x12 body blocks, column-major inside a
+//           block, rows in CSR order (row_ptr / bcol), both triangles stored
+//   contacts[cap]     i32x4 {kind, a, b, 0} sorted by (kind, a, b)
+#pragma once
+#include "common.cuh"
+#include <string>
+#include <vector>
+
+#define CUDA_TRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { \
+    E->fail(ABD_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); return ABD_ERR_CUDA; } } while (0)
+
+// Uniform-grid broad phase over axis-aligned boxes.  Items are stored in the
+// cell of their box's lower corner, hashed into 2^k buckets; the cell edge is
+// the largest box extent of the pass, so a query box covers at most 3 cells
+// per axis.
+struct Grid {
+    int n = 0;                  // stored items
+    int nq = 0;                 // query items
+    int H = 0;                  // buckets (power of two)
+    int bits = 0;
+    float4* lo = nullptr;       // stored boxes (w unused)
+    float4* hi = nullptr;
+    int* scene = nullptr;       // scene of each stored item
+    float4* qlo = nullptr;      // query boxes
+    float4* qhi = nullptr;
+    int* qscene = nullptr;
+    float* cell = nullptr;      // device scalar, cell edge
+    uint32_t* keys = nullptr; uint32_t* keys_s = nullptr;
+    int* vals = nullptr; int* vals_s = nullptr;
+    int* bstart = nullptr; int* bend = nullptr;
+    int* qcount = nullptr;      // nq + 1
+    int* qoff = nullptr;        // nq + 1
+};
+
+struct GridView {
+    const float4* lo; const float4* hi; const int* scene;
+    const float* cell; const int* vals; const int* bstart; const int* bend; uint32_t mask;
+};
+
+DV uint32_t cell_hash(int scene, int cx, int cy, int cz) {
+    return ((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u) ^ ((uint32_t)cz * 83492791u) ^
+           ((uint32_t)scene * 2654435761u);
+}
+
+// Visit every stored item whose box overlaps [qlo,qhi] in the same scene,
+// each exactly once.
+template <class F>
+DV void grid_visit(const GridView& G, float4 qlo, float4 qhi, int scene, F&& visit) {
+    float h = *G.cell;
+    // non-finite boxes (a diverged state) visit nothing; the Newton loop's
+    // NaN check reports them.  The cell edge bounds every box extent, so a
+    // finite query spans at most 3 cells per axis.
+    if (!(h > 0.f && h < 3.0e38f)) return;
+    if (!(isfinite(qlo.x) && isfinite(qlo.y) && isfinite(qlo.z) && isfinite(qhi.x) && isfinite(qhi.y) && isfinite(qhi.z))) return;
+    float fx0 = floorf((qlo.x - h) / h), fx1 = floorf(qhi.x / h);
+    float fy0 = floorf((qlo.y - h) / h), fy1 = floorf(qhi.y / h);
+    float fz0 = floorf((qlo.z - h) / h), fz1 = floorf(qhi.z / h);
+    if (fx1 - fx0 > 4.f || fy1 - fy0 > 4.f || fz1 - fz0 > 4.f) return;
+    if (fabsf(fx0) > 1.0e9f || fabsf(fy0) > 1.0e9f || fabsf(fz0) > 1.0e9f) return;
+    int x0 = (int)fx0, x1 = (int)fx1, y0 = (int)fy0, y1 = (int)fy1, z0 = (int)fz0, z1 = (int)fz1;
+    for (int cz = z0; cz <= z1; cz++)
+        for (int cy = y0; cy <= y1; cy++)
+            for (int cx = x0; cx <= x1; cx++) {
+                uint32_t key = cell_hash(scene, cx, cy, cz) & G.mask;
+                int b = G.bstart[key];
+                if (b < 0) continue;
+                int e = G.bend[key];
+                for (int k = b; k < e; k++) {
+                    int j = G.vals[k];
+                    if (G.scene[j] != scene) continue;
+                    float4 lo = G.lo[j];
+                    if ((int)floorf(lo.x / h) != cx || (int)floorf(lo.y / h) != cy || (int)floorf(lo.z / h) != cz) continue;
+                    float4 hi = G.hi[j];
+                    if (lo.x > qhi.x || hi.x < qlo.x || lo.y > qhi.y || hi.y < qlo.y || lo.z > qhi.z || hi.z < qlo.z) continue;
+                    visit(j);
+                }
+            }
+}
+
+// device counters (one struct in device memory, mirrored in pinned memory)
+struct Counters {
+    int n_ee, n_pt, n_pg, n_total;
+    int overflow, nnzb, n_active, scenes_done;
+    int krylov_active, ccd_capped, nan_flag, ls_pending;
+    int nkeys, pad[3];
+};
+
+struct Engine {
+    AbdParams P;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int ns = 0, nb = 0, nv = 0, ne = 0, nt = 0, npl = 0;
+    bool mixed = false;
+    std::string err;
+    int launches = 0;
+
+    // host-side scene offsets
+    std::vector<int> h_body_begin, h_vert_begin, h_edge_begin, h_tri_begin, h_plane_begin;
+
+    // geometry
+    double* xbar = nullptr; int* vbody = nullptr; int* vscene = nullptr; int* bscene = nullptr;
+    int2* edges = nullptr; int* tris = nullptr; double* mass = nullptr; double* J = nullptr;
+    double* planes = nullptr; int* plane_scene = nullptr; int* sc_plane_begin = nullptr; int* sc_body_begin = nullptr;
+    int* edge_scene = nullptr; int* tri_scene = nullptr;
+
+    // state
+    double* st = nullptr; double* backup = nullptr; double* du = nullptr; double* g = nullptr;
+    double* x = nullptr; float4* xf = nullptr; double* pv = nullptr; double* ws = nullptr;
+    int has_ws = 0;
+
+    // broad phase
+    Grid gee, gpt;                 // EE: edges vs edges; PT: triangles vs points
+    int cap = 0;
+    int4* contacts = nullptr;      // sorted candidate list
+    int4* cst = nullptr;           // stencil vertex ids (-1 padded)
+    int* ctype = nullptr;          // stencil type or -1 inactive
+    double* cxb = nullptr;         // barrier argument
+    int2* cbody = nullptr;         // bodies (b0, b1) of the stencil
+    int4* cblk = nullptr;          // block indices (b0b0, b0b1, b1b0, b1b1)
+
+    // block matrix
+    unsigned long long* keys = nullptr; unsigned long long* keys_s = nullptr; unsigned long long* ukeys = nullptr;
+    int blk_cap = 0;
+    int* row_ptr = nullptr; int* bcol = nullptr;
+    void* vals = nullptr;          // double or float [blk_cap*144]
+    void* dinv = nullptr;          // [nb*144]
+
+    // Krylov vectors (double or float) [12 nb] each
+    void* kv[10] = {nullptr};
+    // per-scene scalars
+    double* scd = nullptr;         // [NSCD][ns]
+    int* sci = nullptr;            // [NSCI][ns]
+
+    // cub scratch
+    void* cub_tmp = nullptr; size_t cub_bytes = 0;
+
+    Counters* dcnt = nullptr; Counters* hcnt = nullptr;   // device / pinned host
+    double* hscd = nullptr; int* hsci = nullptr;          // pinned mirrors of per-scene scalars
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    double* prof_d = nullptr;      // [2][ns][newton_max_iter] residual / alpha of the current step
+    std::vector<int> h_edges, h_tris;  // host copies (global vertex ids) for abd_get_pairs
+
+    // profile of the last abd_step call
+    std::vector<std::vector<double>> prof_res, prof_alpha;
+    std::vector<std::vector<int>> prof_iters;
+
+    int fail(int code, const std::string& m) { err = m; return code; }
+};
+
+// per-scene double slots (scd[slot*ns + s])
+enum {
+    SD_RES = 0, SD_GG, SD_ALPHA, SD_E0, SD_E1, SD_TOI, SD_BB,
+    SD_K0, SD_K1 = SD_K0 + 3, SD_K2 = SD_K1 + 3, SD_K3 = SD_K2 + 3, SD_K4 = SD_K3 + 3, SD_K5 = SD_K4 + 3,
+    SD_KS, SD_KA, SD_KW,            // BiCGSTAB running scalars rho, alpha, omega (even iterations)
+    SD_KR, SD_KR1, SD_KR2,          // the same for odd iterations
+    SD_PAD,
+    SD_COUNT
+};
+// per-scene int slots
+enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_COUNT };
+
+// launch helpers
+inline int grid_for(long n, int block = 256) {
+    long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > NUM_SMS * 16) g = NUM_SMS * 16;
+    return (int)g;
+}
+#define GS_LOOP(i, n) for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (long)(n); i += (long)gridDim.x * blockDim.x)
+
+// implemented in the .cu files
+int eng_alloc(Engine* E);
+void eng_free(Engine* E);
+int eng_transform(Engine* E);
+int eng_detect(Engine* E, double filt);               // sorted candidate list at the nxt state
+int eng_energy(Engine* E, int slot);                   // per-scene energy into scd[slot]
+int eng_assemble(Engine* E);                           // g and blocks at the nxt state (uses the candidate list)
+int eng_solve(Engine* E, int* iters);                  // du = A^-1 g for scenes not done
+int eng_ccd(Engine* E, const double* dq, double sign); // per-scene toi into scd[SD_TOI]
+int eng_step(Engine* E, int n_steps, AbdStepStats* stats);
+int eng_intersections(Engine* E, int* count);
+int eng_sync_counters(Engine* E);

@@ -1,0 +1,196 @@
+// step.cu — the Newton step (abd.py:674-702) with the reference's
+// back-off line search (gauss_newton.py:98-115) and forward_states
+// (abd.py:574-581), run for all scenes of a batch at once.  Each scene keeps
+// its own iteration count, residual, step length and done flag on the
+// device; the host only reads "how many scenes are still iterating".
+#include "engine.cuh"
+
+int eng_energy_masked(Engine* E, int slot, const int* skip);
+
+// nxt.c / nxt.q are 12 consecutive doubles in DoF order [c, q0, q1, q2]
+__global__ void k_backup(int nb, const double* __restrict__ st, double* backup) {
+    GS_LOOP(i, 12L * nb) backup[i] = st[ST_STRIDE * (i / 12) + ST_NXT + (i % 12)];
+}
+// abd.py:768-785: nxt = backup - alpha du, for scenes not yet accepted
+__global__ void k_apply(int nb, const double* __restrict__ backup, const double* __restrict__ du,
+                        const double* __restrict__ alpha, const int* __restrict__ skip, const int* __restrict__ bscene,
+                        double* st) {
+    GS_LOOP(i, 12L * nb) {
+        long b = i / 12;
+        int s = bscene[b];
+        if (skip[s]) continue;
+        st[ST_STRIDE * b + ST_NXT + (i % 12)] = __fma_rn(-alpha[s], du[i], backup[i]);
+    }
+}
+__global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, const double* toi, int ccd) {
+    GS_LOOP(s, ns) {
+        acc[s] = done[s];
+        alpha[s] = ccd ? fmin(1.0, toi[s]) : 1.0;
+    }
+}
+// gauss_newton.py:107-113
+__global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, double min_alpha,
+                            Counters* cnt) {
+    __shared__ int pending;
+    if (threadIdx.x == 0) pending = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        if (acc[s]) continue;
+        if (E1[s] < E0[s]) acc[s] = 1;
+        else if (alpha[s] * 0.5 < min_alpha) acc[s] = 1;
+        else { alpha[s] *= 0.5; atomicAdd(&pending, 1); }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cnt->ls_pending = pending;
+}
+// abd.py:693-699 bookkeeping: record (residual, alpha), stop on tol or cap
+__global__ void k_newton_book(int ns, int* done, int* iter, const double* gg, const double* alpha, double* prof_res,
+                              double* prof_alpha, int max_iter, double tol, Counters* cnt) {
+    __shared__ int ndone, nan;
+    if (threadIdx.x == 0) { ndone = 0; nan = 0; }
+    __syncthreads();
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        if (!done[s]) {
+            int it = iter[s];
+            double res = sqrt(gg[s]);
+            if (!(res == res)) atomicAdd(&nan, 1);
+            prof_res[(long)s * max_iter + it] = res;
+            prof_alpha[(long)s * max_iter + it] = alpha[s];
+            iter[s] = it + 1;
+            if (res < tol || it + 1 >= max_iter || !(res == res)) done[s] = 1;
+        }
+        if (done[s]) atomicAdd(&ndone, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { cnt->scenes_done = ndone; if (nan) cnt->nan_flag = 1; }
+}
+// abd.py:574-581
+__global__ void k_forward(int nb, double* st, double dt) {
+    GS_LOOP(b, nb) {
+        double* s = st + ST_STRIDE * b;
+#pragma unroll
+        for (int k = 0; k < 3; k++) s[ST_NXT + ST_V + k] = (s[ST_NXT + ST_C + k] - s[ST_NOW + ST_C + k]) / dt;
+#pragma unroll
+        for (int k = 0; k < 9; k++) s[ST_NXT + ST_QD + k] = (s[ST_NXT + ST_Q + k] - s[ST_NOW + ST_Q + k]) / dt;
+#pragma unroll
+        for (int k = 0; k < 24; k++) s[ST_NOW + k] = s[ST_NXT + k];
+    }
+}
+// warm start: nxt = now + a * ws (dynamic bodies), a = min(1, toi) per scene
+__global__ void k_ws_apply(int nb, double* st, const double* __restrict__ ws, const double* __restrict__ toi,
+                           const int* __restrict__ bscene, const double* __restrict__ mass, int ccd) {
+    GS_LOOP(i, 12L * nb) {
+        long b = i / 12;
+        if (!(mass[b] > 0.0)) continue;
+        double a = ccd ? fmin(1.0, toi[bscene[b]]) : 1.0;
+        st[ST_STRIDE * b + ST_NXT + (i % 12)] = st[ST_STRIDE * b + ST_NOW + (i % 12)] + a * ws[i];
+    }
+}
+
+int eng_grow_contacts(Engine* E, int need);
+
+int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
+    cudaStream_t s = E->stream;
+    const AbdParams& P = E->P;
+    int ns = E->ns, rc;
+    int* done = E->sci + SI_DONE * ns;
+    int* iter = E->sci + SI_ITER * ns;
+    int* acc = E->sci + SI_ACC * ns;
+    double* alpha = E->scd + SD_ALPHA * ns;
+    int mi = P.newton_max_iter;
+    double* prof_res = E->prof_d;
+    double* prof_alpha = E->prof_d + (long)ns * mi;
+    E->prof_res.assign(ns, {}); E->prof_alpha.assign(ns, {}); E->prof_iters.assign(ns, {});
+    AbdStepStats st; memset(&st, 0, sizeof st); st.min_toi = 1.0;
+    int launches0 = E->launches;
+    CUDA_TRY(cudaEventRecord(E->ev0, s));
+    for (int step = 0; step < n_steps; step++) {
+        CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int) * ns, s));
+        CUDA_TRY(cudaMemsetAsync(iter, 0, sizeof(int) * ns, s));
+        CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, sizeof(Counters), s));
+        if (E->has_ws) {
+            if (P.ccd && (rc = eng_ccd(E, E->ws, 1.0))) return rc;
+            k_ws_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->ws, E->scd + SD_TOI * ns, E->bscene, E->mass, P.ccd);
+            E->launches++;
+            E->has_ws = 0;
+        }
+        for (int it = 0; it < mi; it++) {
+            // contact.py:270-279 detection on the current iterate
+            for (;;) {
+                if ((rc = eng_detect(E, P.cand_dist))) return rc;
+                if ((rc = eng_sync_counters(E))) return rc;
+                if (!E->hcnt->overflow) break;
+                if ((rc = eng_grow_contacts(E, E->hcnt->n_total))) return rc;
+            }
+            st.n_pairs = E->hcnt->n_total;
+            // abd.py:682-688 assembly
+            if ((rc = eng_assemble(E))) return rc;
+            // abd.py:690 / :631-658 solve
+            int li = 0;
+            if ((rc = eng_solve(E, &li))) return rc;
+            st.lin_iters += li;
+            st.n_active = E->hcnt->n_active;
+            // gauss_newton.py:98-115 line search
+            if ((rc = eng_energy_masked(E, SD_E0, done))) return rc;
+            k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
+            E->launches++;
+            if (P.ccd) {
+                if ((rc = eng_ccd(E, E->du, -1.0))) return rc;
+            }
+            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
+            E->launches++;
+            for (int trial = 0; trial < 64; trial++) {
+                k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
+                if ((rc = eng_energy_masked(E, SD_E1, acc))) return rc;
+                k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, P.ls_min_alpha, E->dcnt);
+                E->launches += 2;
+                st.ls_trials++;
+                if ((rc = eng_sync_counters(E))) return rc;
+                if (E->hcnt->ls_pending == 0) break;
+            }
+            k_newton_book<<<1, 256, 0, s>>>(ns, done, iter, E->scd + SD_GG * ns, alpha, prof_res, prof_alpha, mi,
+                                            P.newton_tol, E->dcnt);
+            E->launches++;
+            if ((rc = eng_sync_counters(E))) return rc;
+            if (E->hcnt->nan_flag) return E->fail(ABD_ERR_NAN, "non-finite gradient norm");
+            if (E->hcnt->scenes_done == ns) break;
+        }
+        if (P.ccd) {
+            double* toi = E->scd + SD_TOI * ns;
+            CUDA_TRY(cudaMemcpyAsync(E->hscd, toi, sizeof(double) * ns, cudaMemcpyDeviceToHost, s));
+        }
+        k_forward<<<grid_for(E->nb), 256, 0, s>>>(E->nb, E->st, P.dt);
+        E->launches++;
+        // profile
+        std::vector<double> hr((size_t)ns * mi), ha((size_t)ns * mi);
+        std::vector<int> hi(ns);
+        CUDA_TRY(cudaMemcpyAsync(hr.data(), prof_res, sizeof(double) * ns * mi, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(ha.data(), prof_alpha, sizeof(double) * ns * mi, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(hi.data(), iter, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        for (int sc = 0; sc < ns; sc++) {
+            int n = hi[sc];
+            for (int k = 0; k < n; k++) {
+                E->prof_res[sc].push_back(hr[(size_t)sc * mi + k]);
+                E->prof_alpha[sc].push_back(ha[(size_t)sc * mi + k]);
+            }
+            E->prof_iters[sc].push_back(n);
+            st.newton_iters += n;
+            if (n > st.max_newton_iters) st.max_newton_iters = n;
+            double last = n ? hr[(size_t)sc * mi + n - 1] : 0.0;
+            if (!(last < P.newton_tol)) st.unconverged++;
+            if (last > st.last_residual) st.last_residual = last;
+            if (P.ccd && E->hscd[sc] < st.min_toi) st.min_toi = E->hscd[sc];
+        }
+        st.steps++;
+    }
+    CUDA_TRY(cudaEventRecord(E->ev1, s));
+    CUDA_TRY(cudaEventSynchronize(E->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+    st.gpu_ms = ms;
+    st.kernel_launches = E->launches - launches0;
+    if (stats) *stats = st;
+    if (E->hcnt->ccd_capped) return E->fail(ABD_ERR_CCD_CAP, "CCD iteration cap reached (step clamped conservatively)");
+    return ABD_OK;
+}

@@ -1,0 +1,222 @@
+/*
+ * abd_b200.h — C ABI of libabd_b200.so, the B200 (sm_100a) affine-body-dynamics
+ * Newton step with IPC-style barrier contact.
+ *
+ * The reference exposes this path as the Python class `NewtonAbd`
+ * (abd.py:583-757 of Luke-Skycrawler/colb) driven by `step()` from the viewer
+ * (viewer.py:44-47).  Every entry point below names the reference interface
+ * it replaces.  There is no plugin registry in the reference: a caller picks
+ * the solver by constructing the class (links.py:17-22).
+ *
+ * Conventions
+ *  - Plain C types only.  All arrays are host pointers unless stated.
+ *  - Every call returns an int status (ABD_OK == 0, negative on error).  No
+ *    exception crosses the ABI; abd_last_error() gives the message.
+ *  - One handle per host thread.  All device work runs on the handle's own
+ *    CUDA stream; calls return after that stream is synchronised.
+ *  - Body state layout is the reference's BDFAffine (BDF1.py:11-14 with
+ *    AffineState from quat_util.py:40-47): 48 doubles per body,
+ *        now.c[3] now.q[9] now.v[3] now.qdot[9]  nxt.c[3] nxt.q[9] nxt.v[3] nxt.qdot[9]
+ *    q is row-major with rows = affine DoFs (q = A^T), so a vertex maps as
+ *    x = q^T xbar + c (abd_simple.py:26-35).
+ *  - Per-body DoF vector (gradient, Newton increment): 12 doubles
+ *    [c(3), q row0(3), q row1(3), q row2(3)], body-major (abd.py:595, :780-785).
+ */
+#ifndef ABD_B200_H
+#define ABD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ABD_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define ABD_OK                   0
+#define ABD_ERR_INVALID_ARG     -1
+#define ABD_ERR_CUDA            -2
+#define ABD_ERR_CONTACT_OVERFLOW -3  /* more candidate pairs than capacity (reference wraps silently, contact.py:137) */
+#define ABD_ERR_NAN             -4  /* non-finite energy / gradient / state */
+#define ABD_ERR_SOLVER_CAP      -5  /* Krylov iteration cap hit without reaching tolerance (non-fatal, reported) */
+#define ABD_ERR_NEWTON_CAP      -6  /* Newton iteration cap hit (non-fatal, reported; abd.py:699 stops silently) */
+#define ABD_ERR_CCD_CAP         -7  /* CCD iteration cap hit: step clamped conservatively */
+#define ABD_ERR_NO_DEVICE       -8
+#define ABD_ERR_NOT_BUILT       -9
+
+/* ---- enums ----------------------------------------------------------- */
+/* barrier.py:6-65 — the three barriers of barrier.py, all in x = d^2 */
+#define ABD_BARRIER_CUBIC      0   /* b = -(x-xh)^3          (barrier.py:47-65, the active one) */
+#define ABD_BARRIER_QUADRATIC  1   /* b = (x-xh)^2           (barrier.py:23-44) */
+#define ABD_BARRIER_LOG        2   /* b = -(x-xh)^2 ln(x/xh)/xh^2 (barrier.py:6-21, derivatives as written) */
+
+#define ABD_HESS_REFERENCE     0   /* abd.py:247-251: PSD-project the EE distance Hessian only, PE raw, PP drops B'H */
+#define ABD_HESS_PROJECTED     1   /* project each contact's whole barrier Hessian and each body's ortho Hessian to PSD */
+
+#define ABD_SOLVER_BICGSTAB    0   /* abd.py:636 uses bicgstab; here block-Jacobi preconditioned */
+#define ABD_SOLVER_PCG         1   /* block-Jacobi PCG */
+
+#define ABD_PREC_FP64          0
+#define ABD_PREC_MIXED         1   /* FP32 block matrix + Krylov vectors; FP64 distances, CCD, energy, residual */
+
+/* contact kinds stored in the sorted contact list */
+#define ABD_CONTACT_EE         0   /* edge-edge (contact.py:143-169) */
+#define ABD_CONTACT_PT         1   /* point-triangle (no reference counterpart) */
+#define ABD_CONTACT_PG         2   /* point-half-space (ground / box wall; no reference counterpart) */
+
+/* ---- solver parameters (one set per handle, shared by all scenes) ---- */
+typedef struct AbdParams {
+    double dt;              /* links.py:16 (8e-3) */
+    double gravity[3];      /* abd.py:28, :164-166 ((0,-10,0)) */
+    double kappa;           /* contact stiffness, abd.py:30 (4e8) */
+    double k_ortho;         /* orthogonality stiffness, ortho.py:5 (1e5) */
+    double dhat;            /* barrier activation distance, barrier.py:4-5 (0.095) */
+    double cand_dist;       /* EE candidate filter, contact.py:168 ((thickness+buffer)*2 = 0.19) */
+    int32_t barrier;        /* ABD_BARRIER_* */
+    int32_t hess_mode;      /* ABD_HESS_* */
+    int32_t contact_ee;     /* enable edge-edge contacts */
+    int32_t contact_pt;     /* enable point-triangle contacts */
+    int32_t self_contact;   /* allow pairs within one body (reference: yes, contact.py:160) */
+    int32_t ee_f32;         /* 1: EE filter/classification/barrier distance in FP32 exactly as
+                               contact.py:166 / abd.py:190; 0: FP64 closest points */
+    int32_t linear_solver;  /* ABD_SOLVER_* */
+    int32_t lin_max_iter;   /* Krylov iteration cap per Newton iteration */
+    double lin_tol;         /* relative residual tolerance, abd.py:636 (1e-5) */
+    double newton_tol;      /* ||gradient||_2 tolerance, abd.py:699 (1e-5) */
+    int32_t newton_max_iter;/* abd.py:679 (16) */
+    int32_t ccd;            /* 1: additive-CCD time of impact bounds the line search */
+    double ccd_scale;       /* ACCD conservative rescaling s in (0,1) (0.1 typical) */
+    double ls_min_alpha;    /* gauss_newton.py:110: stop halving when alpha*0.5 < this (1e-2) */
+    int32_t precision;      /* ABD_PREC_* */
+    int32_t contact_capacity;/* max candidate pairs per detection (reference: 10000, contact.py:8) */
+    double pinned_diag;     /* diagonal of pinned bodies' blocks, abd.py:146 (100) */
+    int32_t warm_start;     /* 1: start Newton from nxt = now + user increment (abd_set_warm_start) */
+    int32_t reserved[7];
+} AbdParams;
+
+/* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */
+typedef struct AbdSceneDesc {
+    int32_t n_bodies;
+    int32_t n_verts;
+    int32_t n_edges;
+    int32_t n_tris;
+    const double*  xbar;       /* n_verts*3 rest positions in the body frame (Soup.xcs) */
+    const int32_t* vert_body;  /* n_verts body index, 0-based within this scene (Soup.body) */
+    const int32_t* edges;      /* n_edges*2 vertex indices (Soup.edges) */
+    const int32_t* tris;       /* n_tris*3 vertex indices (Soup.triangles) */
+    const double*  mass;       /* n_bodies, m<=0 pins the body (abd.py:115, rbd_simple.py:42-48) */
+    const double*  inertia_J;  /* n_bodies scalar J of M = diag(m,J,J,J) (x) I3 (abd.py:77-85) */
+    const double*  state;      /* n_bodies*48 initial BDFAffine (abd_simple.py:37-49) */
+    int32_t n_planes;          /* static half-spaces n.x >= offset (ground, box walls) */
+    const double*  planes;     /* n_planes*4 : nx ny nz offset (n unit) */
+} AbdSceneDesc;
+
+/* ---- per-step statistics -------------------------------------------- */
+typedef struct AbdStepStats {
+    int32_t steps;             /* steps taken by this call */
+    int32_t newton_iters;      /* sum over steps and scenes of Newton iterations */
+    int32_t max_newton_iters;  /* max over steps/scenes */
+    int32_t lin_iters;         /* total Krylov iterations */
+    int32_t n_pairs;           /* candidate pairs at the last detection */
+    int32_t n_active;          /* active (d < dhat) contacts at the last assembly */
+    int32_t unconverged;       /* (step,scene) pairs that hit the Newton cap */
+    int32_t ls_trials;         /* total line-search energy evaluations */
+    double  last_residual;     /* max over scenes of the last Newton iteration's ||g|| */
+    double  min_toi;           /* smallest CCD time of impact seen (1 if none) */
+    double  gpu_ms;            /* device time of the call (CUDA events) */
+    int32_t kernel_launches;   /* kernels launched by the call */
+    int32_t reserved[5];
+} AbdStepStats;
+
+typedef struct AbdHandle AbdHandle;
+
+/* Fills p with the reference's constants (abd.py:27-30, barrier.py:4-5,
+ * contact.py:7-9, ortho.py:5, links.py:16, gauss_newton.py:110). */
+void abd_default_params(AbdParams* p);
+
+/* Replaces NewtonAbd.__init__ (abd.py:584-599) together with
+ * ContactSolverBase.__init__ (contact.py:204-241) and AbdComplex/JSONComplex
+ * scene set-up (abd_simple.py:53-69): copies the scene to the device and
+ * allocates every buffer the step needs.  n_scenes > 1 builds a batch of
+ * independent scenes stepped together (no reference counterpart). */
+int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_scenes,
+               int32_t device, AbdHandle** out);
+
+/* Frees all device memory of the handle. */
+int abd_destroy(AbdHandle* h);
+
+/* Size queries. */
+int abd_get_sizes(AbdHandle* h, int32_t* n_bodies, int32_t* n_verts, int32_t* n_edges,
+                  int32_t* n_tris, int32_t* n_scenes);
+
+/* Replaces assigning NewtonAbd.history (abd_simple.py:14, :64-69). */
+int abd_set_state(AbdHandle* h, const double* bdf_affine, int32_t n_bodies);
+/* Replaces NewtonAbd.history.numpy() (BDFAffine array, 48 doubles/body). */
+int abd_get_state(AbdHandle* h, double* bdf_affine_out);
+
+/* Replaces NewtonAbd.step() (abd.py:674-702): n_steps full Newton steps with
+ * collision detection, assembly, linear solve, line search and
+ * forward_states.  stats may be NULL. */
+int abd_step(AbdHandle* h, int32_t n_steps, AbdStepStats* stats);
+
+/* Per-(step, Newton-iteration) profile of the last abd_step call for scene
+ * `scene`: residual ||g|| and accepted alpha, like Profiller.convergence /
+ * .alphas (abd.py:695-696, utils/data_collector.py:4-55).  Writes at most
+ * cap entries; *n gets the number of iterations recorded. */
+int abd_get_profile(AbdHandle* h, int32_t scene, double* residuals, double* alphas,
+                    int32_t* iters_per_step, int32_t cap, int32_t* n);
+
+/* Replaces compute_V(ret=True) (abd_simple.py:71-78): vertex positions of
+ * the nxt state, n_verts*3 doubles. */
+int abd_get_vertices(AbdHandle* h, double* x_out);
+
+/* Runs detection on the current nxt state and returns the sorted candidate
+ * list (replaces ContactSolverBase.detect_collision, contact.py:270-279).
+ * Each entry is 4 vertex indices (XConstraint.a1a2b1b2, contact.py:46-51)
+ * for EE; for PT (p, t0, t1, t2); for PG (p, plane, -1, -1).  kinds_out
+ * (may be NULL) gets ABD_CONTACT_* per entry.  Order: kind, then first
+ * primitive index, then second. */
+int abd_get_pairs(AbdHandle* h, int32_t* out4, int32_t* kinds_out, int32_t cap, int32_t* n);
+
+/* Replaces get_contact_points (abd.py:748-766): midpoint and distance per
+ * candidate pair (EE closest points), cap entries. */
+int abd_get_contact_points(AbdHandle* h, double* points_out, double* dists_out,
+                           int32_t cap, int32_t* n);
+
+/* Total incremental potential of the nxt state per scene (replaces
+ * NewtonAbd.compute_g, abd.py:725-735). */
+int abd_energy(AbdHandle* h, double* energy_per_scene);
+
+/* Assembles gradient and Hessian at the nxt state (abd.py:686-688 with the
+ * triplet overlap of the reference fixed) and copies them out: grad is
+ * n_bodies*12; hess_dense (may be NULL) is (12 n_bodies)^2 row-major and
+ * is only allowed for n_bodies <= 512. */
+int abd_assemble(AbdHandle* h, double* grad, double* hess_dense);
+
+/* Newton increment du = H^-1 g of the current assembly (abd.py:631-658);
+ * du is n_bodies*12.  *iters gets the Krylov iteration count. */
+int abd_solve(AbdHandle* h, double* du, int32_t* iters);
+
+/* Warm start: per-body 12-DoF increment added to nxt = now at the start of
+ * the next step (no reference counterpart; used by the learned warm start).
+ * Values are in DoF order [c, q0, q1, q2]; the increment is clipped by CCD. */
+int abd_set_warm_start(AbdHandle* h, const float* dq12, int32_t n_bodies);
+
+/* Per-body features for the learned warm start: 48 floats per body
+ * (q 9, qdot 9, q_tilde 12, contact count 1, 8 smallest contact distances ... ). */
+int abd_get_features(AbdHandle* h, float* feat_out, int32_t n_bodies);
+
+/* Number of edge-triangle intersections between different bodies at the
+ * nxt state (FP64 exact predicate); 0 means intersection-free. */
+int abd_count_intersections(AbdHandle* h, int32_t* count);
+
+/* Message of the last failing call on this handle (or a global one for NULL). */
+const char* abd_last_error(AbdHandle* h);
+
+int abd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABD_B200_H */

@@ -1,0 +1,159 @@
+"""CUDA path vs the CPU oracle on the same seeded inputs (needs a GPU).
+
+Bit-exact: vertex transform, candidate pair sets (float32 EE predicate and
+float64 PT / half-space filters).  FP64 tolerances: energy 1e-11 rel,
+gradient / Hessian 1e-9 rel, trajectories 1e-6 rel of the scene extent
+(the north-star FP64 bar).  Mixed precision: 1e-4.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from colb_b200 import params as P, scene as S
+from colb_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def _edge_pairs(sc, quads):
+    key = {(a, b): i for i, (a, b) in enumerate(sc["edges"])}
+    return np.array([(key[(q[0], q[1])], key[(q[2], q[3])]) for q in quads], dtype=np.int32).reshape(-1, 2)
+
+
+def _pair(params, sc):
+    return Engine(params, sc), O.OracleWorld(params, sc)
+
+
+def test_transform_bitexact(chain_scene, chain_pairs):
+    e, o = _pair(P.reference_params(), chain_scene)
+    for k in range(3):
+        e.set_state(chain_pairs["states"][k]); o.set_state(chain_pairs["states"][k])
+        assert np.array_equal(e.vertices(), o.vertices())
+
+
+def test_chain_pairs_bitexact_vs_golden(chain_scene, chain_pairs):
+    e = Engine(P.reference_params(), chain_scene)
+    for k in range(3):
+        e.set_state(chain_pairs["states"][k])
+        quads, kinds = e.pairs()
+        assert np.all(kinds == 0)
+        assert np.array_equal(_edge_pairs(chain_scene, quads), chain_pairs[f"pairs{k}"])
+
+
+@pytest.mark.parametrize("which", ["cubes", "net"])
+def test_config_pairs_match_oracle(which):
+    sc = S.config1_cubes(seed=3) if which == "cubes" else S.config2_chain_net(n=3, seed=1)
+    p = P.config_params(cand_dist=0.05)
+    e, o = _pair(p, sc)
+    st = sc["state"].copy()
+    rng = np.random.default_rng(5)
+    st[:, 24:27] += rng.normal(scale=0.05, size=(len(st), 3))
+    e.set_state(st); o.set_state(st)
+    qe, ke = e.pairs(); qo, ko = o.pairs()
+    assert np.array_equal(ke, ko) and np.array_equal(qe, qo)
+
+
+def test_energy_matches_oracle(chain_scene, chain_pairs):
+    e, o = _pair(P.reference_params(), chain_scene)
+    for k in range(3):
+        e.set_state(chain_pairs["states"][k]); o.set_state(chain_pairs["states"][k])
+        assert e.energy()[0] == pytest.approx(o.energy()[0], rel=1e-11)
+
+
+@pytest.mark.parametrize("hess_mode", [0, 1])
+def test_assembly_matches_oracle(chain_scene, chain_pairs, hess_mode):
+    p = P.reference_params(hess_mode=hess_mode)
+    e, o = _pair(p, chain_scene)
+    st = chain_pairs["states"][2]
+    e.set_state(st); o.set_state(st)
+    ge, He = e.assemble(); go, Ho = o.assemble()
+    assert np.abs(ge - go).max() <= 1e-9 * np.abs(go).max()
+    assert np.abs(He - Ho).max() <= 1e-9 * np.abs(Ho).max()
+
+
+def test_assembly_config_contacts():
+    sc = S.config1_cubes(seed=2)
+    st = sc["state"].copy()
+    st[:4, 25] -= st[:4, 25] - 0.5 * np.sqrt(3) + 0.0  # drop the lower layer near the ground
+    p = P.config_params(dhat=0.3, cand_dist=0.3)
+    e, o = _pair(p, sc)
+    e.set_state(st); o.set_state(st)
+    ge, He = e.assemble(); go, Ho = o.assemble()
+    assert np.abs(go).max() > 0
+    assert np.abs(ge - go).max() <= 1e-9 * np.abs(go).max()
+    assert np.abs(He - Ho).max() <= 1e-9 * np.abs(Ho).max()
+
+
+@pytest.mark.parametrize("solver", [0, 1])
+def test_solve_matches_dense(chain_scene, chain_pairs, solver):
+    p = P.reference_params(linear_solver=solver, lin_tol=1e-12, hess_mode=1)
+    e, o = _pair(p, chain_scene)
+    st = chain_pairs["states"][1]
+    e.set_state(st); o.set_state(st)
+    du, it = e.solve()
+    g, H = o.assemble()
+    ref = np.linalg.solve(H, g)
+    assert np.abs(du - ref).max() <= 1e-8 * np.abs(ref).max()
+    assert it > 0
+
+
+def test_reference_chain_trajectory(chain_scene):
+    p = P.reference_params(lin_tol=1e-10)
+    e, o = _pair(p, chain_scene)
+    for _ in range(4):
+        rc, se = e.step(5)
+        o.step(5)
+        xe, xo = e.vertices(), o.vertices()
+        scale = np.abs(xo).max()
+        assert np.abs(xe - xo).max() <= 1e-6 * scale
+    assert se.unconverged == 0
+
+
+def test_config_cubes_trajectory_and_no_intersection():
+    sc = S.config1_cubes(seed=0)
+    p = P.config_params(lin_tol=1e-10)
+    e, o = _pair(p, sc)
+    for _ in range(3):
+        e.step(10); o.step(10)
+        xe, xo = e.vertices(), o.vertices()
+        assert np.abs(xe - xo).max() <= 1e-6 * np.abs(xo).max()
+        assert e.count_intersections() == 0
+
+
+def test_batch_equals_single_scenes():
+    scenes = S.config3_batch(n_scenes=4, seed=7, nmin=4, nmax=8)
+    p = P.config_params(lin_tol=1e-10)
+    eb = Engine(p, scenes)
+    eb.step(3)
+    sb = eb.get_state()
+    off = 0
+    for sc in scenes:
+        e = Engine(p, sc)
+        e.step(3)
+        n = len(sc["mass"])
+        assert np.abs(e.get_state() - sb[off:off + n]).max() <= 1e-9 * max(1.0, np.abs(sb).max())
+        off += n
+
+
+def test_mixed_precision_close_to_fp64(chain_scene):
+    e64 = Engine(P.reference_params(lin_tol=1e-9), chain_scene)
+    e32 = Engine(P.reference_params(lin_tol=1e-6, precision=1), chain_scene)
+    e64.step(10); e32.step(10)
+    x64, x32 = e64.vertices(), e32.vertices()
+    assert np.abs(x64 - x32).max() <= 1e-4 * np.abs(x64).max()
+
+
+def test_contact_capacity_grows(chain_scene, chain_pairs):
+    e = Engine(P.reference_params(contact_capacity=64), chain_scene)
+    e.set_state(chain_pairs["states"][2])
+    quads, _ = e.pairs()
+    assert np.array_equal(_edge_pairs(chain_scene, quads), chain_pairs["pairs2"])
+
+
+def test_invalid_arguments_return_errors(chain_scene):
+    from colb_b200.engine import AbdError
+    with pytest.raises(AbdError):
+        Engine(P.reference_params(dhat=-1.0), chain_scene)
+    e = Engine(P.reference_params(), chain_scene)
+    with pytest.raises(AbdError):
+        e.set_state(np.zeros((e.nb + 1, 48)).ravel()[: 48 * e.nb].reshape(e.nb, 48)[:-1])
