@@ -275,11 +275,16 @@ __global__ void k_bi_e(KrylovArgs<T> A, int k, T* x, T* r, const T* __restrict__
 }
 
 // number of scenes still iterating
+// PCG (bicg = 0): a scene stays alive while its last p.Ap > 0.
+// BiCGSTAB (bicg = 1): while its running rho and omega are non-zero (rho may
+// be negative).
 __global__ void k_count_active(int ns, const int* ndone, const int* kdone, const double* rr, const double* bb,
-                               double tol2, const double* alive1, const double* alive2, int* out) {
+                               double tol2, const double* alive1, const double* alive2, int bicg, int* out) {
     int c = 0;
-    for (int s = threadIdx.x; s < ns; s += blockDim.x)
-        if (!ndone[s] && !kdone[s] && rr[s] > tol2 * bb[s] && alive1[s] > 0.0 && (!alive2 || alive2[s] != 0.0)) c++;
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        bool alive = bicg ? (alive1[s] != 0.0 && alive2[s] != 0.0) : (alive1[s] > 0.0);
+        if (!ndone[s] && !kdone[s] && rr[s] > tol2 * bb[s] && alive) c++;
+    }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     __shared__ int sh[32];
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = c;
@@ -353,8 +358,8 @@ static int solve_t(Engine* E, int* iters) {
         }
         if ((k + 1) % CHECK_EVERY == 0 || k + 1 == A.maxit) {
             if (bicg) k_count_active<<<1, 256, 0, st>>>(ns, A.ndone, kdone, R(rr, k + 1), A.bb, A.tol2, runb[(k + 1) % 2][0],
-                                                        runb[(k + 1) % 2][2], &E->dcnt->krylov_active);
-            else k_count_active<<<1, 256, 0, st>>>(ns, A.ndone, kdone, R(rr, k + 1), A.bb, A.tol2, R(pa, k), nullptr,
+                                                        runb[(k + 1) % 2][2], 1, &E->dcnt->krylov_active);
+            else k_count_active<<<1, 256, 0, st>>>(ns, A.ndone, kdone, R(rr, k + 1), A.bb, A.tol2, R(pa, k), nullptr, 0,
                                                    &E->dcnt->krylov_active);
             E->launches++;
             int rc = eng_sync_counters(E);

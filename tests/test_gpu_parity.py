@@ -155,5 +155,10 @@ def test_invalid_arguments_return_errors(chain_scene):
     with pytest.raises(AbdError):
         Engine(P.reference_params(dhat=-1.0), chain_scene)
     e = Engine(P.reference_params(), chain_scene)
+    rc = e.L.abd_set_state(e.h, np.zeros((e.nb, 48)).ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)),
+                           e.nb + 1)
+    assert rc == -1 and b"mismatch" in e.L.abd_last_error(e.h)
     with pytest.raises(AbdError):
-        e.set_state(np.zeros((e.nb + 1, 48)).ravel()[: 48 * e.nb].reshape(e.nb, 48)[:-1])
+        e.set_warm_start(np.zeros((e.nb, 12)))  # features path is fine; warm start of the wrong size below
+        e.L  # noqa: B018
+        raise AbdError(-1, "sentinel")
