@@ -1,0 +1,301 @@
+"""Benchmark: ABD body-steps/s at the 1e-5 Newton residual (plus Newton
+iterations per step) for one workload, as one JSON line.
+
+Workloads (--workload):
+  net16   16x16 chain mail of 256 torus links (288 verts / 576 tris each),
+          corner links pinned, dt = 1/240, FP64 (default; the chain-net
+          configuration of the benchmark suite)
+  chain   the reference's own 144-link chain scene with its constants
+  cubes   8 falling unit cubes on a ground plane, dt = 1/120
+  batch   512 independent scenes of 4..64 cubes/tori, one handle
+A step is one physics time step of the whole workload (Newton to 1e-5 or
+16 iterations, with collision detection, assembly, Krylov solve, CCD and
+line search).  Inputs are seeded synthetic scenes.
+
+Arms: --impl ours (default) runs libabd_b200.so; --impl reference runs the
+CPU restatement of the reference's step (the oracle: the reference itself
+is Python + NVIDIA Warp, which is not installable here) on all host cores.
+
+Multi-GPU (torchrun): every rank steps its own replica (seeded by rank) on
+its own GPU with no collective in the step ("replicas only" for single-scene
+workloads; scenes shard for `batch`); the value is all ranks' body-steps
+over the slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "ABD body-steps/s @1e-5 residual: learned+batched vs plain, same B200; iters/step"
+
+
+def make_workload(name, rank=0, precision=0, ns_batch=512):
+    from colb_b200 import params as P, scene as S
+    if name == "net16":
+        sc = S.config2_chain_net(n=16, seed=rank)
+        p = P.config_params(dt=1.0 / 240.0, precision=precision)
+        cfg = dict(workload="net16: 16x16 torus chain mail, 256 links (R 1.0, r 0.25, 24x12 -> 288 v / 576 t), "
+                   "4 corners pinned, dt 1/240, log barrier dhat 1e-3 kappa 1e7, k_ortho 1e7, CCD line search",
+                   bodies=256, verts=len(sc["xbar"]), tris=len(sc["tris"]))
+        return [sc], p, cfg
+    if name == "chain":
+        sc = S.load_npz_scene(os.path.join(ROOT, "tests", "golden", "chains_scene.npz"))
+        p = P.reference_params(precision=precision)
+        cfg = dict(workload="chain: reference assets/chains.json, 144 links of link.ma, reference constants "
+                   "(dt 8e-3, kappa 4e8, cubic barrier dhat 0.095, EE contact)", bodies=144, verts=len(sc["xbar"]))
+        return [sc], p, cfg
+    if name == "cubes":
+        sc = S.config1_cubes(seed=rank)
+        p = P.config_params(precision=precision)
+        cfg = dict(workload="cubes: 8 unit cubes 2x2x2, ground plane, dt 1/120", bodies=8)
+        return [sc], p, cfg
+    if name == "batch":
+        scenes = S.config3_batch(n_scenes=ns_batch, seed=rank)
+        p = P.config_params(precision=precision)
+        nb = sum(len(s["mass"]) for s in scenes)
+        cfg = dict(workload=f"batch: {ns_batch} scenes of 4..64 cubes/tori (log-uniform), ground, dt 1/120",
+                   bodies=nb, scenes=ns_batch)
+        return scenes, p, cfg
+    raise SystemExit(f"unknown workload {name}")
+
+
+def dynamic_bodies(scenes):
+    return int(sum((s["mass"] > 0).sum() for s in scenes))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        return d.get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_baseline(scenes, params, cfg, budget_s=20.0, threads=None):
+    """The oracle (CPU restatement of the reference step) on all host cores,
+    on a bounded sample of the same workload: the full scene for as many
+    steps as fit in about `budget_s`."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count()
+    O.set_threads(threads)
+    w = O.OracleWorld(params, scenes)
+    nb = dynamic_bodies(scenes)
+    steps, t0 = 0, time.perf_counter()
+    iters = 0
+    while True:
+        rc, st = w.step(1)
+        steps += 1
+        iters += st.newton_iters
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 200:
+            break
+    value = nb * steps / el
+    return {"value": value, "unit": "body-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} full steps of {cfg['workload'].split(':')[0]} from t=0 ({el:.1f} s, "
+                      f"{iters / max(1, steps * len(scenes)):.2f} Newton iters/step/scene), oracle/abd_oracle.c with OpenMP"}
+
+
+def flush_l2(buf):
+    buf.add_(1.0)   # writes 256 MB (> 126 MB L2)
+
+
+def run_ours(args, rank, world):
+    import torch
+    from colb_b200.engine import Engine
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    scenes, p, cfg = make_workload(args.workload, rank, args.precision)
+    eng = Engine(p, scenes, device=dev)
+    nb = dynamic_bodies(scenes)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        eng.step(1)
+    # ---- timed: device time of K steps, L2 flushed before each step
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    gpu_ms, launches, iters, unconv, lin = 0.0, 0, 0, 0, 0
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            rc, st = eng.step(1)
+            gpu_ms += st.gpu_ms
+            launches += st.kernel_launches
+            iters += st.newton_iters
+            unconv += st.unconverged
+            lin += st.lin_iters
+    torch.cuda.synchronize()
+    t = torch.tensor([gpu_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    # ---- e2e through the public API with host buffers: H2D of the state,
+    # one step, D2H of the state every step
+    host_state = eng.get_state()
+    try:
+        pinned = torch.from_numpy(host_state).pin_memory().numpy()
+    except Exception:
+        pinned = host_state
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.set_state(pinned)
+        eng.step(1)
+        pinned[:] = eng.get_state()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    # ---- per-phase device timers (separate pass, same workload state)
+    eng.set_timing(True, True)
+    n_timing = max(2, min(args.steps, 5))
+    for _ in range(n_timing):
+        eng.step(1)
+    phases = eng.timing()
+    eng.set_timing(False, True)
+    return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
+                lin=lin, e2e_s=float(e2e_t.item()), clocks=clk.summary(), phases=phases, n_timing=n_timing,
+                bytes_state=48 * 8 * eng.nb)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="net16", choices=["net16", "chain", "cubes", "batch"])
+    ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed FP32/FP64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        scenes, p, cfg = make_workload(args.workload, 0, args.precision)
+        cb = cpu_baseline(scenes, p, cfg, budget_s=max(10.0, 6.0 * args.steps))
+        line = {"metric": METRIC, "value": cb["value"], "unit": "body-steps/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": cfg, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "reference = CPU restatement of abd.py's step (the reference needs NVIDIA Warp, not installable here)"}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    r = run_ours(args, rank, world)
+    nb_total = r["nb"] * world
+    value = nb_total * args.steps / (r["max_ms"] / 1000.0)
+    e2e = nb_total * args.steps / r["e2e_s"]
+    peak, peak_kind = measured_peaks()
+    ph = r["phases"]
+    # dominant kernel class among the individually timed ones
+    dom = max(("spmv", "energy_query"), key=lambda k: ph[k]["ms"])
+    avg_ms = ph[dom]["ms"] / max(1, ph[dom]["launches"])
+    avg_bytes = ph[dom]["bytes"] / max(1, ph[dom]["launches"])
+    achieved = avg_bytes / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["max_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f32+f64",
+        "data": "synthetic",
+        "config": dict(r["cfg"], parallelism=f"replicas x{world}" if args.workload != "batch" else f"scenes sharded x{world}",
+                       l2="flushed before every timed step (256 MB write)", precision="fp64" if args.precision == 0 else "mixed"),
+        "newton_iters_per_step": r["iters"] / (args.steps * len(r["scenes"])),
+        "krylov_iters_per_step": r["lin"] / args.steps,
+        "unconverged_steps": r["unconv"],
+        "gpu_launches": r["launches"],
+        "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": r["bytes_state"],
+                "d2h_bytes_per_step": r["bytes_state"]},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic_from_profiles(dom, args.workload),
+                     "algorithmic_bytes_per_launch": avg_bytes, "avg_launch_ms": avg_ms},
+        "phases_ms_per_step": {k: v["ms"] / r["n_timing"] for k, v in ph.items()},
+        "clocks": r["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(r["scenes"], r["p"], r["cfg"])
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -285,6 +285,7 @@ int eng_assemble(Engine* E) {
     E->launches += 4;
     if ((rc = eng_sync_counters(E))) return rc;
     int nnzb = E->hcnt->nkeys;   // may include the sentinel
+    E->nnzb_host = nnzb;
     if (nnzb > E->blk_cap) { if ((rc = eng_grow_blocks(E, nnzb))) return rc; }
     k_block_rows<<<grid_for(nnzb), 256, 0, s>>>(nb, E->ukeys, n_unique, E->row_ptr, E->bcol, E->dcnt);
     double sc = P.kappa * P.dt * P.dt;

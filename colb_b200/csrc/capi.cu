@@ -483,3 +483,51 @@ int abd_count_intersections(AbdHandle* h, int32_t* count) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ phase timers
+static cudaEvent_t pool_get(Engine* E) {
+    if (!E->ev_pool.empty()) { cudaEvent_t e = E->ev_pool.back(); E->ev_pool.pop_back(); return e; }
+    cudaEvent_t e; cudaEventCreate(&e); return e;
+}
+int phase_begin(Engine* E, int phase) {
+    if (!E->timing) return -1;
+    Engine::Rec r; r.phase = phase; r.a = pool_get(E); r.b = pool_get(E); r.bytes = 0;
+    cudaEventRecord(r.a, E->stream);
+    E->recs.push_back(r);
+    return (int)E->recs.size() - 1;
+}
+void phase_end(Engine* E, int rec, double bytes) {
+    if (rec < 0 || !E->timing) return;
+    E->recs[rec].bytes = bytes;
+    cudaEventRecord(E->recs[rec].b, E->stream);
+}
+void phase_collect(Engine* E) {
+    for (auto& r : E->recs) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            E->phase_ms[r.phase] += ms; E->phase_n[r.phase] += 1; E->phase_bytes[r.phase] += r.bytes;
+        }
+        E->ev_pool.push_back(r.a); E->ev_pool.push_back(r.b);
+    }
+    E->recs.clear();
+}
+
+extern "C" int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset) {
+    HANDLE(h);
+    cudaStreamSynchronize(E->stream);
+    phase_collect(E);
+    E->timing = on != 0;
+    if (reset) for (int i = 0; i < ABD_NUM_PHASES; i++) { E->phase_ms[i] = 0; E->phase_n[i] = 0; E->phase_bytes[i] = 0; }
+    return ABD_OK;
+}
+extern "C" int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes) {
+    HANDLE(h);
+    cudaStreamSynchronize(E->stream);
+    phase_collect(E);
+    for (int i = 0; i < ABD_NUM_PHASES; i++) {
+        if (ms) ms[i] = E->phase_ms[i];
+        if (launches) launches[i] = E->phase_n[i];
+        if (bytes) bytes[i] = E->phase_bytes[i];
+    }
+    return ABD_OK;
+}

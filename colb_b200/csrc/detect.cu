@@ -499,15 +499,21 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
     if (P.contact_ee && E->ne > 1) {
         if ((rc = build_ee_grid(E, P.dhat))) return rc;
         Grid& g = E->gee;
+        int ph = phase_begin(E, PH_EQUERY);
         k_ee_energy<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, view(g), G, g.lo, g.hi, g.scene, P.ee_f32, P.self_contact,
                                                           P.dhat, P.barrier, sc, skip, Eo);
+        // edges, their boxes/scene, sorted values, bucket table, positions
+        phase_end(E, ph, E->ne * (8.0 + 32.0 + 4.0 + 4.0) + g.H * 8.0 + E->nv * (P.ee_f32 ? 16.0 : 24.0));
         E->launches++;
     }
     if (P.contact_pt && E->nt > 0) {
         if ((rc = build_pt_grid(E, P.dhat))) return rc;
         Grid& g = E->gpt;
+        int ph = phase_begin(E, PH_EQUERY);
         k_pt_energy<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, view(g), G, g.qlo, g.qhi, g.qscene, P.self_contact, P.dhat,
                                                           P.barrier, sc, skip, Eo);
+        // points and their boxes, triangles, their boxes/scene, sorted values, buckets, positions
+        phase_end(E, ph, E->nv * (32.0 + 4.0 + 24.0) + E->nt * (12.0 + 32.0 + 4.0 + 4.0) + g.H * 8.0);
         E->launches++;
     }
     if (E->npl > 0) {

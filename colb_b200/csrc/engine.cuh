@@ -130,6 +130,7 @@ struct Engine {
     // block matrix
     unsigned long long* keys = nullptr; unsigned long long* keys_s = nullptr; unsigned long long* ukeys = nullptr;
     int blk_cap = 0;
+    int nnzb_host = 0;             // block count of the last assembly (host copy)
     int* row_ptr = nullptr; int* bcol = nullptr;
     void* vals = nullptr;          // double or float [blk_cap*144]
     void* dinv = nullptr;          // [nb*144]
@@ -155,8 +156,25 @@ struct Engine {
     std::vector<std::vector<double>> prof_res, prof_alpha;
     std::vector<std::vector<int>> prof_iters;
 
+    // phase timers
+    bool timing = false;
+    struct Rec { int phase; cudaEvent_t a, b; double bytes; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> ev_pool;
+    double phase_ms[ABD_NUM_PHASES] = {0};
+    long long phase_n[ABD_NUM_PHASES] = {0};
+    double phase_bytes[ABD_NUM_PHASES] = {0};
+
     int fail(int code, const std::string& m) { err = m; return code; }
 };
+
+enum { PH_DETECT = 0, PH_ASSEMBLE, PH_SOLVE, PH_ENERGY, PH_CCD, PH_OTHER, PH_EQUERY, PH_SPMV };
+
+// Bracket device work with events when timing is on.  phase_begin returns a
+// record index (or -1), phase_end closes it with the algorithmic bytes moved.
+int phase_begin(Engine* E, int phase);
+void phase_end(Engine* E, int rec, double bytes);
+void phase_collect(Engine* E);   // after a stream sync: fold finished records into the totals
 
 // per-scene double slots (scd[slot*ns + s])
 enum {

@@ -328,6 +328,9 @@ static int solve_t(Engine* E, int* iters) {
     // SD_KS..SD_KR slots hold buffer 0, the K5 ring's spare slots buffer 1)
     double* runb[2][3] = {{E->scd + SD_KS * ns, E->scd + SD_KA * ns, E->scd + SD_KW * ns},
                           {E->scd + SD_KR * ns, E->scd + (SD_KR + 1) * ns, E->scd + (SD_KR + 2) * ns}};
+    // algorithmic bytes of one SpMV: every block once, the input vector
+    // (and for PCG the previous direction) once, two output vectors
+    double spmv_bytes = (double)sizeof(T) * (144.0 * E->nnzb_host + 48.0 * nb);
     int k = 0;
     for (; k < A.maxit; k++) {
         if (!bicg) {
@@ -335,8 +338,10 @@ static int solve_t(Engine* E, int* iters) {
             T* pcur = kv[(k % 2) ? KV_P1 : KV_P0];
             if (k == 0) { pprev = kv[KV_P0]; pcur = kv[KV_P0]; }
             // K1 zeros rz/rr slot k+1; K2 zeros pAp slot k+1
+            int ph = phase_begin(E, PH_SPMV);
             k_pcg_spmv<T><<<grid, nthr, 0, st>>>(A, k, kv[KV_Z], pprev, pcur, kv[KV_V], R(rz, k), R(rz, k + 2), R(rr, k),
                                                  R(pa, k + 2), R(pa, k), R(rz, k + 1), R(rr, k + 1));
+            phase_end(E, ph, spmv_bytes);
             k_pcg_update<T><<<grid, nthr, 0, st>>>(A, k, kv[KV_X], kv[KV_R], kv[KV_Z], pcur, kv[KV_V], R(rz, k), R(pa, k),
                                                    R(rr, k), R(pa, k + 2), R(rz, k + 1), R(rr, k + 1), R(pa, k + 1), kiter);
             E->launches += 2;
@@ -347,7 +352,9 @@ static int solve_t(Engine* E, int* iters) {
             k_bi_a<T><<<grid, nthr, 0, st>>>(A, k, kv[KV_R], kv[KV_P0], kv[KV_V], kv[KV_Y], R(rz, k), R(rr, k), rc_[0], rc_[1],
                                              rc_[2], R(pa, k), R(s1, k), R(s2, k), R(s3, k), R(rz, k + 1));
             CUDA_TRY(cudaMemsetAsync(R(rr, k + 1), 0, sizeof(double) * ns, st));
+            int ph = phase_begin(E, PH_SPMV);
             k_bi_spmv<T><<<grid, nthr, 0, st>>>(A, k, kv[KV_Y], kv[KV_V], kv[KV_RH], R(pa, k), nullptr, R(rr, k), rc_[0], rc_[2]);
+            phase_end(E, ph, spmv_bytes);
             k_bi_c<T><<<grid, nthr, 0, st>>>(A, k, kv[KV_X], kv[KV_R], kv[KV_V], kv[KV_Y], kv[KV_S], kv[KV_Z], R(rz, k),
                                              R(pa, k), R(rr, k), R(s1, k), rc_[0], rc_[2]);
             k_bi_spmv<T><<<grid, nthr, 0, st>>>(A, k, kv[KV_Z], kv[KV_T], kv[KV_S], R(s2, k), R(s3, k), R(rr, k), rc_[0], rc_[2]);

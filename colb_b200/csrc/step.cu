@@ -89,6 +89,16 @@ __global__ void k_ws_apply(int nb, double* st, const double* __restrict__ ws, co
 
 int eng_grow_contacts(Engine* E, int need);
 
+// algorithmic bytes of one detection: positions in, float copy out, per
+// edge/triangle/point the box, key, value, count and offset traffic, the
+// bucket table, and the pair list written
+static double detect_bytes(Engine* E) {
+    double b = E->nv * (24.0 + 24.0 + 16.0);
+    b += E->ne * (8.0 + 32.0 + 4.0 + 4.0 * 4 + 8.0) + E->gee.H * 8.0;
+    if (E->P.contact_pt) b += E->nt * (12.0 + 32.0 + 16.0) + E->nv * (32.0 + 8.0) + E->gpt.H * 8.0;
+    return b;
+}
+
 int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
@@ -117,31 +127,35 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
         for (int it = 0; it < mi; it++) {
             // contact.py:270-279 detection on the current iterate
             for (;;) {
-                if ((rc = eng_detect(E, P.cand_dist))) return rc;
+                int ph = phase_begin(E, PH_DETECT);
+                rc = eng_detect(E, P.cand_dist);
+                phase_end(E, ph, detect_bytes(E));
+                if (rc) return rc;
                 if ((rc = eng_sync_counters(E))) return rc;
                 if (!E->hcnt->overflow) break;
                 if ((rc = eng_grow_contacts(E, E->hcnt->n_total))) return rc;
             }
             st.n_pairs = E->hcnt->n_total;
             // abd.py:682-688 assembly
-            if ((rc = eng_assemble(E))) return rc;
+            { int ph = phase_begin(E, PH_ASSEMBLE); rc = eng_assemble(E); phase_end(E, ph, 0); if (rc) return rc; }
             // abd.py:690 / :631-658 solve
             int li = 0;
-            if ((rc = eng_solve(E, &li))) return rc;
+            { int ph = phase_begin(E, PH_SOLVE); rc = eng_solve(E, &li); phase_end(E, ph, 0); if (rc) return rc; }
             st.lin_iters += li;
             st.n_active = E->hcnt->n_active;
             // gauss_newton.py:98-115 line search
-            if ((rc = eng_energy_masked(E, SD_E0, done))) return rc;
+            { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_masked(E, SD_E0, done); phase_end(E, ph, 0); if (rc) return rc; }
             k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
             E->launches++;
             if (P.ccd) {
-                if ((rc = eng_ccd(E, E->du, -1.0))) return rc;
+                int ph = phase_begin(E, PH_CCD); rc = eng_ccd(E, E->du, -1.0); phase_end(E, ph, 0);
+                if (rc) return rc;
             }
             k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
             E->launches++;
             for (int trial = 0; trial < 64; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
-                if ((rc = eng_energy_masked(E, SD_E1, acc))) return rc;
+                { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_masked(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
                 k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, P.ls_min_alpha, E->dcnt);
                 E->launches += 2;
                 st.ls_trials++;
@@ -186,6 +200,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     }
     CUDA_TRY(cudaEventRecord(E->ev1, s));
     CUDA_TRY(cudaEventSynchronize(E->ev1));
+    phase_collect(E);
     float ms = 0;
     cudaEventElapsedTime(&ms, E->ev0, E->ev1);
     st.gpu_ms = ms;

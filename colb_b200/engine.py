@@ -20,8 +20,9 @@ EXPORTS = [
     "abd_default_params", "abd_create", "abd_destroy", "abd_get_sizes", "abd_set_state", "abd_get_state",
     "abd_step", "abd_get_profile", "abd_get_vertices", "abd_get_pairs", "abd_get_contact_points",
     "abd_energy", "abd_assemble", "abd_solve", "abd_set_warm_start", "abd_get_features",
-    "abd_count_intersections", "abd_last_error", "abd_abi_version",
+    "abd_count_intersections", "abd_last_error", "abd_abi_version", "abd_set_timing", "abd_get_timing",
 ]
+PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv"]
 
 
 class AbdError(RuntimeError):
@@ -60,6 +61,8 @@ def load_library(path=LIB_PATH):
     L.abd_last_error.argtypes = [vp]
     L.abd_last_error.restype = C.c_char_p
     L.abd_abi_version.argtypes = []
+    L.abd_set_timing.argtypes = [vp, C.c_int32, C.c_int32]
+    L.abd_get_timing.argtypes = [vp, dp, C.POINTER(C.c_int64), dp]
     _lib = L
     return L
 
@@ -176,6 +179,14 @@ class Engine:
         f = np.zeros((self.nb, 48), dtype=np.float32)
         self._check(self.L.abd_get_features(self.h, f.ctypes.data_as(C.POINTER(C.c_float)), self.nb))
         return f
+
+    def set_timing(self, on=True, reset=True):
+        self._check(self.L.abd_set_timing(self.h, int(on), int(reset)))
+
+    def timing(self):
+        ms = np.zeros(len(PHASES)); n = np.zeros(len(PHASES), dtype=np.int64); by = np.zeros(len(PHASES))
+        self._check(self.L.abd_get_timing(self.h, _dp(ms), n.ctypes.data_as(C.POINTER(C.c_int64)), _dp(by)))
+        return {PHASES[i]: dict(ms=float(ms[i]), launches=int(n[i]), bytes=float(by[i])) for i in range(len(PHASES))}
 
     def count_intersections(self):
         n = C.c_int32()

@@ -303,28 +303,40 @@ def config1_cubes(seed=0, spacing=1.05):
     return assemble_bodies(bodies, planes=[GROUND])
 
 
-def config2_chain_net(n=16, seed=0, pitch=1.5, R=1.0, r=0.25, nu=24, nv=12, vel_noise=1e-3):
-    """n x n net of torus links in the xz plane, pitch apart.  Links on even
-    (i+j) lie flat (axis y); links on odd (i+j) stand up with their plane
-    containing x (odd i) or z (even i), so each standing link threads its
-    flat neighbours along that axis.  The four corner links are pinned;
-    every other link gets a seeded +-vel_noise initial velocity."""
+def config2_chain_net(n=16, seed=0, pitch=1.48, R=1.0, r=0.25, nu=24, nv=12, vel_noise=1e-3, lift=0.9):
+    """n x n net of torus links in the xz plane, `pitch` apart, built as
+    square chain mail:
+      * (even, even) sites: flat links (axis y);
+      * (odd, even) sites: standing links in the xy plane, each threading
+        its two flat neighbours along x;
+      * (even, odd) sites: standing links in the yz plane, threading along z;
+      * (odd, odd) sites: flat links raised by `lift`, resting on the mail.
+    Standing links are the 90-degree rotations of the flat ones about the
+    grid axes.  Two interlocked links whose centres are 2(R - r) = 1.5 apart
+    touch with zero gap, so the default pitch of 1.48 leaves a 0.02 gap.
+    The four corner links are pinned; every other link gets a seeded
+    +-vel_noise initial velocity."""
     rng = np.random.default_rng(seed)
-    V, F = torus_mesh(R, r, nu, nv)           # ring in xy plane (axis z)
-    flat = np.array([[1, 0, 0], [0, 0, -1], [0, 1, 0]], dtype=np.float64)   # axis z -> y
-    stand_x = np.eye(3)                                                      # xy plane
-    stand_z = np.array([[0, 0, 1], [0, 1, 0], [-1, 0, 0]], dtype=np.float64)  # zy plane
+    V, F = torus_mesh(R, r, nu, nv)           # ring in the xy plane (axis z)
+    flat = np.array([[1, 0, 0], [0, 0, -1], [0, 1, 0]], dtype=np.float64)    # axis z -> y
+    stand_x = np.eye(3)                                                       # xy plane
+    stand_z = np.array([[0, 0, 1], [0, 1, 0], [-1, 0, 0]], dtype=np.float64)  # yz plane
     bodies = []
     corners = {(0, 0), (0, n - 1), (n - 1, 0), (n - 1, n - 1)}
     for i in range(n):
         for j in range(n):
-            if (i + j) % 2 == 0:
+            y = 0.0
+            if i % 2 == 0 and j % 2 == 0:
                 Rm = flat
+            elif i % 2 == 1 and j % 2 == 0:
+                Rm = stand_x
+            elif i % 2 == 0 and j % 2 == 1:
+                Rm = stand_z
             else:
-                Rm = stand_x if i % 2 == 1 else stand_z
+                Rm, y = flat, lift
             pinned = (i, j) in corners
             v = np.zeros(3) if pinned else rng.uniform(-vel_noise, vel_noise, 3)
-            bodies.append(_body(V, F, 1000.0, [i * pitch, 0.0, j * pitch], Rm, v=v, pinned=pinned))
+            bodies.append(_body(V, F, 1000.0, [i * pitch, y, j * pitch], Rm, v=v, pinned=pinned))
     return assemble_bodies(bodies)
 
 

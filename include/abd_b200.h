@@ -211,6 +211,20 @@ int abd_get_features(AbdHandle* h, float* feat_out, int32_t n_bodies);
  * nxt state (FP64 exact predicate); 0 means intersection-free. */
 int abd_count_intersections(AbdHandle* h, int32_t* count);
 
+/* Device-side phase timers (no reference counterpart; the reference wraps
+ * step() in wp.ScopedTimer, abd.py:676).  When on, every phase launch is
+ * bracketed by CUDA events on the handle's stream and summed per phase:
+ *   0 detect (transform, grid, pair list)   1 assemble (blocks, gradient)
+ *   2 solve (Krylov)                        3 line-search energy
+ *   4 CCD                                   5 other (bookkeeping, forward)
+ *   6 contact-energy query kernels only     7 SpMV kernels only
+ * abd_get_timing writes ms[8], launches[8] and the algorithmic bytes[8]
+ * those phases moved (see the library's documentation of each kernel);
+ * reset clears them. */
+#define ABD_NUM_PHASES 8
+int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset);
+int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes);
+
 /* Message of the last failing call on this handle (or a global one for NULL). */
 const char* abd_last_error(AbdHandle* h);
 
