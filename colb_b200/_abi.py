@@ -19,7 +19,7 @@ ABD_ERR_NOT_BUILT = -9
 
 BARRIER_CUBIC, BARRIER_QUADRATIC, BARRIER_LOG = 0, 1, 2
 HESS_REFERENCE, HESS_PROJECTED = 0, 1
-SOLVER_BICGSTAB, SOLVER_PCG = 0, 1
+SOLVER_BICGSTAB, SOLVER_PCG, SOLVER_DIRECT, SOLVER_AUTO = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 CONTACT_EE, CONTACT_PT, CONTACT_PG = 0, 1, 2
 

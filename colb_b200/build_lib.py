@@ -54,7 +54,7 @@ def build(verbose=False, extra=()):
             if err.strip():
                 print(err)
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart_static"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart_static", "-lcusolver", "-lcublas"]
         subprocess.check_call(cmd)
     return OUT
 

@@ -44,6 +44,8 @@ static void grid_free(Grid& G) {
 
 static size_t cub_need(Engine* E, int nkeys64) {
     size_t need = 0, b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, E->sw_cap + 1);
+    need = std::max(need, b);
     int nmax = std::max(std::max(E->ne, E->nt), 1);
     cub::DeviceRadixSort::SortPairs(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, (int*)nullptr, (int*)nullptr, nmax);
     need = std::max(need, b);
@@ -85,6 +87,20 @@ int eng_grow_contacts(Engine* E, int need) {
     return ABD_OK;
 }
 
+int eng_grow_swept(Engine* E, int need) {
+    int cap = std::max(need + need / 4 + 1024, 2 * E->sw_cap);
+    cudaStreamSynchronize(E->stream);
+    void* ps[] = {E->sw, E->sw_flag, E->sw_off, E->cub_tmp};
+    for (void* p : ps) if (p) cudaFree(p);
+    E->sw = nullptr; E->sw_flag = nullptr; E->sw_off = nullptr; E->cub_tmp = nullptr;
+    E->sw_cap = cap;
+    DALLOC(E->sw, cap); DALLOC(E->sw_flag, cap + 1); DALLOC(E->sw_off, cap + 1);
+    E->cub_bytes = cub_need(E, E->nb + 2 * E->cap);
+    if (cudaMalloc(&E->cub_tmp, E->cub_bytes) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc cub scratch");
+    E->sw_valid = false;
+    return ABD_OK;
+}
+
 int eng_alloc(Engine* E) {
     int nb = E->nb, nv = E->nv, ns = E->ns;
     int rc;
@@ -93,7 +109,12 @@ int eng_alloc(Engine* E) {
     DALLOC(E->st, 48L * nb); DALLOC(E->backup, 12L * nb); DALLOC(E->du, 12L * nb); DALLOC(E->g, 12L * nb);
     DALLOC(E->x, 3L * nv); DALLOC(E->xf, nv); DALLOC(E->pv, 3L * nv); DALLOC(E->ws, 12L * nb);
     E->cap = 0;
+    E->sw_cap = std::max(E->P.contact_capacity, 1024);
     if ((rc = eng_grow_contacts(E, std::max(E->P.contact_capacity, 1024) * 4 / 5))) return rc;
+    DALLOC(E->sw, E->sw_cap); DALLOC(E->sw_flag, E->sw_cap + 1); DALLOC(E->sw_off, E->sw_cap + 1);
+    DALLOC(E->pmag, nv); DALLOC(E->zero_int, 1); DALLOC(E->zero_ns, ns);
+    cudaMemsetAsync(E->zero_int, 0, sizeof(int), E->stream);
+    cudaMemsetAsync(E->zero_ns, 0, sizeof(int) * ns, E->stream);
     DALLOC(E->row_ptr, nb + 1);
     E->blk_cap = 0;
     if ((rc = eng_grow_blocks(E, nb + std::min(2 * E->cap, 8 * nb + 1024)))) return rc;
@@ -115,11 +136,13 @@ int eng_alloc(Engine* E) {
 }
 
 void eng_free(Engine* E) {
+    eng_dense_free(E);
     grid_free(E->gee); grid_free(E->gpt);
     void* ps[] = {E->xbar, E->vbody, E->vscene, E->bscene, E->edges, E->tris, E->mass, E->J, E->planes, E->plane_scene,
                   E->sc_plane_begin, E->sc_body_begin, E->edge_scene, E->tri_scene, E->st, E->backup, E->du, E->g, E->x,
                   E->xf, E->pv, E->ws, E->contacts, E->cst, E->ctype, E->cxb, E->cbody, E->cblk, E->keys, E->keys_s,
-                  E->ukeys, E->row_ptr, E->bcol, E->vals, E->dinv, E->scd, E->sci, E->cub_tmp, E->dcnt, E->prof_d};
+                  E->ukeys, E->row_ptr, E->bcol, E->vals, E->dinv, E->scd, E->sci, E->cub_tmp, E->dcnt, E->prof_d,
+                  E->sw, E->sw_flag, E->sw_off, E->pmag, E->zero_int, E->zero_ns};
     for (void* p : ps) if (p) cudaFree(p);
     for (int i = 0; i < 10; i++) if (E->kv[i]) cudaFree(E->kv[i]);
     if (E->hcnt) cudaFreeHost(E->hcnt);
@@ -173,7 +196,7 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     if (device < 0 || device >= ndev) { g_err = "abd_create: bad device index"; return ABD_ERR_INVALID_ARG; }
     const AbdParams& P = *params;
     if (!(P.dt > 0) || !(P.dhat > 0) || !(P.cand_dist >= P.dhat) || P.newton_max_iter <= 0 || P.lin_max_iter <= 0 ||
-        P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1))) {
+        P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || P.linear_solver < 0 || P.linear_solver > 3 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1))) {
         g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale)";
         return ABD_ERR_INVALID_ARG;
     }
@@ -221,6 +244,7 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
         sc_plane_begin.push_back(npl); sc_body_begin.push_back(nb);
     }
     E->nb = nb; E->nv = nv; E->ne = (int)escene.size(); E->nt = (int)tscene.size(); E->npl = npl;
+    E->h_body_begin = sc_body_begin;
     E->h_edges = edges; E->h_tris = tris;
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) { delete E; g_err = "stream"; return ABD_ERR_CUDA; }
     auto up = [&](auto*& dst, auto& src) -> int {
@@ -273,6 +297,7 @@ int abd_set_state(AbdHandle* h, const double* st, int32_t n) {
     if (!st || n != E->nb) return E->fail(ABD_ERR_INVALID_ARG, "abd_set_state: n_bodies mismatch");
     CUDA_TRY(cudaMemcpyAsync(E->st, st, sizeof(double) * 48 * n, cudaMemcpyHostToDevice, E->stream));
     CUDA_TRY(cudaStreamSynchronize(E->stream));
+    E->sw_valid = false;
     return ABD_OK;
 }
 

@@ -35,6 +35,10 @@ __global__ void k_transform(int nv, const double* __restrict__ xbar, const int* 
     }
 }
 
+int eng_body_energy(Engine* E, double* Eo, const int* skip);
+int eng_pg_energy(Engine* E, double* Eo, const int* skip);
+int eng_pg_candidates(Engine* E, double filt);
+
 int eng_transform(Engine* E) {
     k_transform<<<grid_for(E->nv), 256, 0, E->stream>>>(E->nv, E->xbar, E->vbody, E->st, E->x, E->xf);
     E->launches++;
@@ -185,7 +189,7 @@ __global__ void k_grid_ranges(int n, const uint32_t* __restrict__ keys, int* bst
     }
 }
 
-static int grid_build(Engine* E, Grid& G) {
+int eng_grid_build(Engine* E, Grid& G) {
     if (G.n == 0) return ABD_OK;
     cudaStream_t s = E->stream;
     k_cell_floor<<<1, 32, 0, s>>>(G.cell);
@@ -197,7 +201,7 @@ static int grid_build(Engine* E, Grid& G) {
     E->launches += 4;
     return ABD_OK;
 }
-static GridView view(const Grid& G) {
+GridView eng_view(const Grid& G) {
     return GridView{G.lo, G.hi, G.scene, G.cell, G.vals_s, G.bstart, G.bend, (uint32_t)(G.H - 1)};
 }
 
@@ -325,7 +329,7 @@ static int build_ee_grid(Engine* E, double filt) {
     k_edge_boxes<<<grid_for(G.n), 256, 0, E->stream>>>(G.n, E->edges, E->x, E->xf, E->edge_scene, pad, E->P.ee_f32,
                                                        G.lo, G.hi, G.scene, G.cell);
     E->launches++;
-    return grid_build(E, G);
+    return eng_grid_build(E, G);
 }
 static int build_pt_grid(Engine* E, double filt) {
     Grid& G = E->gpt;
@@ -335,41 +339,49 @@ static int build_pt_grid(Engine* E, double filt) {
     k_tri_boxes<<<grid_for(G.n), 256, 0, E->stream>>>(G.n, E->tris, E->x, E->tri_scene, pad, G.lo, G.hi, G.scene, G.cell);
     k_point_boxes<<<grid_for(G.nq), 256, 0, E->stream>>>(G.nq, E->x, E->vscene, pad, G.qlo, G.qhi, G.qscene, G.cell);
     E->launches += 2;
-    return grid_build(E, G);
+    return eng_grid_build(E, G);
 }
 
 int eng_detect(Engine* E, double filt) {
     int rc;
     cudaStream_t s = E->stream;
     if ((rc = eng_transform(E))) return rc;
-    CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, sizeof(Counters), s));
+    CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, DETECT_COUNTER_BYTES, s));
     Geo G = geo(E);
     int f32 = E->P.ee_f32, sc = E->P.self_contact;
     if (E->P.contact_ee && E->ne > 1) {
         if ((rc = build_ee_grid(E, filt))) return rc;
         Grid& g = E->gee;
-        k_ee_pairs<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, view(g), G, g.lo, g.hi, g.scene, f32, sc, filt, 0,
+        k_ee_pairs<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, eng_view(g), G, g.lo, g.hi, g.scene, f32, sc, filt, 0,
                                                          g.qcount, nullptr, 0, E->dcnt, E->cap, E->contacts, &E->dcnt->overflow);
         CUDA_TRY(cudaMemsetAsync(g.qcount + E->ne, 0, sizeof(int), s));
         if ((rc = scan_counts(E, g.qcount, g.qoff, E->ne))) return rc;
         k_store_count<<<1, 32, 0, s>>>(g.qoff, E->ne, 0, E->dcnt);
-        k_ee_pairs<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, view(g), G, g.lo, g.hi, g.scene, f32, sc, filt, 1,
+        k_ee_pairs<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, eng_view(g), G, g.lo, g.hi, g.scene, f32, sc, filt, 1,
                                                          g.qcount, g.qoff, 0, E->dcnt, E->cap, E->contacts, &E->dcnt->overflow);
         E->launches += 3;
     }
     if (E->P.contact_pt && E->nt > 0) {
         if ((rc = build_pt_grid(E, filt))) return rc;
         Grid& g = E->gpt;
-        k_pt_pairs<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, view(g), G, g.qlo, g.qhi, g.qscene, sc, filt, 0,
+        k_pt_pairs<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, eng_view(g), G, g.qlo, g.qhi, g.qscene, sc, filt, 0,
                                                          g.qcount, nullptr, E->dcnt, E->cap, E->contacts, &E->dcnt->overflow);
         CUDA_TRY(cudaMemsetAsync(g.qcount + E->nv, 0, sizeof(int), s));
         if ((rc = scan_counts(E, g.qcount, g.qoff, E->nv))) return rc;
         k_store_count<<<1, 32, 0, s>>>(g.qoff, E->nv, 1, E->dcnt);
-        k_pt_pairs<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, view(g), G, g.qlo, g.qhi, g.qscene, sc, filt, 1,
+        k_pt_pairs<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, eng_view(g), G, g.qlo, g.qhi, g.qscene, sc, filt, 1,
                                                          g.qcount, g.qoff, E->dcnt, E->cap, E->contacts, &E->dcnt->overflow);
         E->launches += 3;
     }
+    return eng_pg_candidates(E, filt);
+}
+
+// half-space candidates appended after EE and PT, then the total
+int eng_pg_candidates(Engine* E, double filt) {
+    cudaStream_t s = E->stream;
+    int rc;
     if (E->npl > 0) {
+        Geo G = geo(E);
         // reuse the PT query buffers for the per-vertex plane counts
         int* qc = E->gpt.qcount; int* qo = E->gpt.qoff;
         k_pg_pairs<<<grid_for(E->nv), 256, 0, s>>>(E->nv, G, E->vscene, filt, 0, qc, nullptr, E->dcnt, E->cap, E->contacts, &E->dcnt->overflow);
@@ -491,16 +503,14 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
     CUDA_TRY(cudaMemsetAsync(Eo, 0, sizeof(double) * E->ns, s));
     if ((rc = eng_transform(E))) return rc;
     const AbdParams& P = E->P;
-    k_body_energy<<<grid_for(E->nb), 256, 0, s>>>(E->nb, E->st, E->mass, E->J, E->bscene, P.dt, P.gravity[0], P.gravity[1],
-                                                  P.gravity[2], P.k_ortho, skip, Eo);
-    E->launches++;
+    if ((rc = eng_body_energy(E, Eo, skip))) return rc;
     double sc = P.kappa * P.dt * P.dt;
     Geo G = geo(E);
     if (P.contact_ee && E->ne > 1) {
         if ((rc = build_ee_grid(E, P.dhat))) return rc;
         Grid& g = E->gee;
         int ph = phase_begin(E, PH_EQUERY);
-        k_ee_energy<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, view(g), G, g.lo, g.hi, g.scene, P.ee_f32, P.self_contact,
+        k_ee_energy<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, eng_view(g), G, g.lo, g.hi, g.scene, P.ee_f32, P.self_contact,
                                                           P.dhat, P.barrier, sc, skip, Eo);
         // edges, their boxes/scene, sorted values, bucket table, positions
         phase_end(E, ph, E->ne * (8.0 + 32.0 + 4.0 + 4.0) + g.H * 8.0 + E->nv * (P.ee_f32 ? 16.0 : 24.0));
@@ -510,14 +520,26 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
         if ((rc = build_pt_grid(E, P.dhat))) return rc;
         Grid& g = E->gpt;
         int ph = phase_begin(E, PH_EQUERY);
-        k_pt_energy<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, view(g), G, g.qlo, g.qhi, g.qscene, P.self_contact, P.dhat,
+        k_pt_energy<<<grid_for(E->nv, 128), 128, 0, s>>>(E->nv, eng_view(g), G, g.qlo, g.qhi, g.qscene, P.self_contact, P.dhat,
                                                           P.barrier, sc, skip, Eo);
         // points and their boxes, triangles, their boxes/scene, sorted values, buckets, positions
         phase_end(E, ph, E->nv * (32.0 + 4.0 + 24.0) + E->nt * (12.0 + 32.0 + 4.0 + 4.0) + g.H * 8.0);
         E->launches++;
     }
+    return eng_pg_energy(E, Eo, skip);
+}
+int eng_body_energy(Engine* E, double* Eo, const int* skip) {
+    const AbdParams& P = E->P;
+    k_body_energy<<<grid_for(E->nb), 256, 0, E->stream>>>(E->nb, E->st, E->mass, E->J, E->bscene, P.dt, P.gravity[0],
+                                                          P.gravity[1], P.gravity[2], P.k_ortho, skip, Eo);
+    E->launches++;
+    return ABD_OK;
+}
+int eng_pg_energy(Engine* E, double* Eo, const int* skip) {
+    const AbdParams& P = E->P;
     if (E->npl > 0) {
-        k_pg_energy<<<grid_for(E->nv), 256, 0, s>>>(E->nv, G, E->vscene, P.dhat, P.barrier, sc, skip, Eo);
+        k_pg_energy<<<grid_for(E->nv), 256, 0, E->stream>>>(E->nv, geo(E), E->vscene, P.dhat, P.barrier,
+                                                            P.kappa * P.dt * P.dt, skip, Eo);
         E->launches++;
     }
     return ABD_OK;
@@ -617,8 +639,8 @@ int eng_ccd(Engine* E, const double* dq, double sign) {
         CUDA_TRY(cudaMemsetAsync(g.cell, 0, sizeof(float), s));
         k_swept_edge_boxes<<<grid_for(g.n), 256, 0, s>>>(g.n, E->edges, E->x, E->pv, E->edge_scene, g.lo, g.hi, g.scene, g.cell);
         E->launches++;
-        if ((rc = grid_build(E, g))) return rc;
-        k_ccd_ee<<<grid_for(E->ne, 64), 64, 0, s>>>(E->ne, view(g), G, E->pv, g.lo, g.hi, g.scene, P.self_contact, P.ccd_scale,
+        if ((rc = eng_grid_build(E, g))) return rc;
+        k_ccd_ee<<<grid_for(E->ne, 64), 64, 0, s>>>(E->ne, eng_view(g), G, E->pv, g.lo, g.hi, g.scene, P.self_contact, P.ccd_scale,
                                                     done, toi, &E->dcnt->ccd_capped);
         E->launches++;
     }
@@ -628,8 +650,8 @@ int eng_ccd(Engine* E, const double* dq, double sign) {
         k_swept_tri_boxes<<<grid_for(g.n), 256, 0, s>>>(g.n, E->tris, E->x, E->pv, E->tri_scene, g.lo, g.hi, g.scene, g.cell);
         k_swept_point_boxes<<<grid_for(g.nq), 256, 0, s>>>(g.nq, E->x, E->pv, E->vscene, g.qlo, g.qhi, g.qscene, g.cell);
         E->launches += 2;
-        if ((rc = grid_build(E, g))) return rc;
-        k_ccd_pt<<<grid_for(E->nv, 64), 64, 0, s>>>(E->nv, view(g), G, E->pv, g.qlo, g.qhi, g.qscene, P.self_contact, P.ccd_scale,
+        if ((rc = eng_grid_build(E, g))) return rc;
+        k_ccd_pt<<<grid_for(E->nv, 64), 64, 0, s>>>(E->nv, eng_view(g), G, E->pv, g.qlo, g.qhi, g.qscene, P.self_contact, P.ccd_scale,
                                                     done, toi, &E->dcnt->ccd_capped);
         E->launches++;
     }
@@ -669,12 +691,12 @@ int eng_intersections(Engine* E, int* count) {
     if ((rc = eng_transform(E))) return rc;
     Grid& g = E->gpt;   // triangles stored; edge boxes as queries (in the EE grid's box arrays)
     CUDA_TRY(cudaMemsetAsync(g.cell, 0, sizeof(float), s));
-    CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, sizeof(Counters), s));
+    CUDA_TRY(cudaMemsetAsync(&E->dcnt->nkeys, 0, sizeof(int), s));
     k_tri_boxes<<<grid_for(g.n), 256, 0, s>>>(g.n, E->tris, E->x, E->tri_scene, 0.f, g.lo, g.hi, g.scene, g.cell);
     Grid& q = E->gee;
     k_edge_boxes<<<grid_for(q.n), 256, 0, s>>>(q.n, E->edges, E->x, E->xf, E->edge_scene, 0.f, 0, q.lo, q.hi, q.scene, g.cell);
-    if ((rc = grid_build(E, g))) return rc;
-    k_intersections<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, view(g), geo(E), q.lo, q.hi, q.scene, &E->dcnt->nkeys);
+    if ((rc = eng_grid_build(E, g))) return rc;
+    k_intersections<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, eng_view(g), geo(E), q.lo, q.hi, q.scene, &E->dcnt->nkeys);
     E->launches += 3;
     CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));

@@ -91,8 +91,10 @@ struct Counters {
     int n_ee, n_pt, n_pg, n_total;
     int overflow, nnzb, n_active, scenes_done;
     int krylov_active, ccd_capped, nan_flag, ls_pending;
-    int nkeys, pad[3];
+    int nkeys, pad0, pad1, pad2;
+    int n_sw, n_sw_ee, sw_overflow, pad3;
 };
+#define DETECT_COUNTER_BYTES (5 * sizeof(int))   // n_ee .. overflow
 
 struct Engine {
     AbdParams P;
@@ -127,6 +129,13 @@ struct Engine {
     int2* cbody = nullptr;         // bodies (b0, b1) of the stencil
     int4* cblk = nullptr;          // block indices (b0b0, b0b1, b1b0, b1b1)
 
+    // swept candidate list (swept.cu)
+    int4* sw = nullptr; int sw_cap = 0; int n_sw = 0, n_sw_ee = 0; bool sw_valid = false;
+    int* sw_flag = nullptr; int* sw_off = nullptr;
+    float* pmag = nullptr;         // |displacement| per vertex of the listed step
+    int* zero_int = nullptr;       // a device 0
+    int* zero_ns = nullptr;        // ns device zeros (no scene skipped)
+
     // block matrix
     unsigned long long* keys = nullptr; unsigned long long* keys_s = nullptr; unsigned long long* ukeys = nullptr;
     int blk_cap = 0;
@@ -150,6 +159,8 @@ struct Engine {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     double* prof_d = nullptr;      // [2][ns][newton_max_iter] residual / alpha of the current step
+    void* dense_state = nullptr;   // direct-solver state (dense.cu)
+    int krylov_kind = ABD_SOLVER_BICGSTAB;
     std::vector<int> h_edges, h_tris;  // host copies (global vertex ids) for abd_get_pairs
 
     // profile of the last abd_step call
@@ -206,7 +217,16 @@ int eng_detect(Engine* E, double filt);               // sorted candidate list a
 int eng_energy(Engine* E, int slot);                   // per-scene energy into scd[slot]
 int eng_assemble(Engine* E);                           // g and blocks at the nxt state (uses the candidate list)
 int eng_solve(Engine* E, int* iters);                  // du = A^-1 g for scenes not done
+int eng_solve_direct(Engine* E, int* iters);           // dense factorization per scene
+void eng_dense_free(Engine* E);
+long long eng_dense_bytes(Engine* E);
 int eng_ccd(Engine* E, const double* dq, double sign); // per-scene toi into scd[SD_TOI]
 int eng_step(Engine* E, int n_steps, AbdStepStats* stats);
 int eng_intersections(Engine* E, int* count);
 int eng_sync_counters(Engine* E);
+int eng_grid_build(Engine* E, Grid& G);
+GridView eng_view(const Grid& G);
+int eng_swept(Engine* E, const double* dq, double sign, const int* done);
+int eng_ccd_list(Engine* E, const int* skip);
+int eng_energy_list(Engine* E, int slot, const int* skip);
+int eng_detect_list(Engine* E);

@@ -15,6 +15,9 @@
 #include "engine.cuh"
 
 #define CHECK_EVERY 8
+
+// resolved Krylov method for one solve
+struct KrylovKind { KrylovKind(Engine* E, int k) { E->krylov_kind = k; } };
 #define HALF 16
 
 // kv slots
@@ -311,7 +314,7 @@ static int solve_t(Engine* E, int* iters) {
     CUDA_TRY(cudaMemsetAsync(kiter, 0, sizeof(int) * ns, st));
     // zero all rings
     CUDA_TRY(cudaMemsetAsync(E->scd + SD_BB * ns, 0, sizeof(double) * ns * (SD_COUNT - SD_BB), st));
-    int bicg = E->P.linear_solver == ABD_SOLVER_BICGSTAB;
+    int bicg = E->krylov_kind == ABD_SOLVER_BICGSTAB;
     int nthr = 256;
     int grid = grid_for((long)nb * HALF, nthr);
     double* rz = E->scd + SD_K0 * ns;   // ring of 3 (PCG rz / BiCGSTAB rho)
@@ -386,6 +389,13 @@ static int solve_t(Engine* E, int* iters) {
 }
 
 int eng_solve(Engine* E, int* iters) {
+    int kind = E->P.linear_solver;
+    if (kind == ABD_SOLVER_AUTO) {
+        bool fits = E->ns <= 64 && eng_dense_bytes(E) <= (4LL << 30);
+        kind = fits ? ABD_SOLVER_DIRECT : (E->P.hess_mode == ABD_HESS_PROJECTED ? ABD_SOLVER_PCG : ABD_SOLVER_BICGSTAB);
+    }
+    if (kind == ABD_SOLVER_DIRECT) return eng_solve_direct(E, iters);
+    KrylovKind kk(E, kind);
     if (E->mixed) return solve_t<float>(E, iters);
     return solve_t<double>(E, iters);
 }

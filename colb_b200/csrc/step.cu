@@ -76,6 +76,16 @@ __global__ void k_forward(int nb, double* st, double dt) {
         for (int k = 0; k < 24; k++) s[ST_NOW + k] = s[ST_NXT + k];
     }
 }
+// inertial prediction as an increment from now: ws = q_tilde - q_now
+__global__ void k_ws_inertial(int nb, const double* __restrict__ st, double dt, double g0, double g1, double g2,
+                              double* ws) {
+    GS_LOOP(i, 12L * nb) {
+        long b = i / 12; int k = (int)(i % 12);
+        const double* now = st + ST_STRIDE * b + ST_NOW;
+        double gv = k == 0 ? g0 : (k == 1 ? g1 : g2);
+        ws[i] = k < 3 ? dt * now[ST_V + k] + dt * dt * gv : dt * now[ST_QD + (k - 3)];
+    }
+}
 // warm start: nxt = now + a * ws (dynamic bodies), a = min(1, toi) per scene
 __global__ void k_ws_apply(int nb, double* st, const double* __restrict__ ws, const double* __restrict__ toi,
                            const int* __restrict__ bscene, const double* __restrict__ mass, int ccd) {
@@ -118,17 +128,25 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
         CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int) * ns, s));
         CUDA_TRY(cudaMemsetAsync(iter, 0, sizeof(int) * ns, s));
         CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, sizeof(Counters), s));
+        if (P.warm_start == 2) {
+            k_ws_inertial<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, P.dt, P.gravity[0], P.gravity[1], P.gravity[2], E->ws);
+            E->launches++;
+            E->has_ws = 1;
+        }
         if (E->has_ws) {
-            if (P.ccd && (rc = eng_ccd(E, E->ws, 1.0))) return rc;
+            // warm start: list and CCD along now -> now + ws, then move
+            if ((rc = eng_swept(E, E->ws, 1.0, done))) return rc;
+            if (P.ccd && (rc = eng_ccd_list(E, done))) return rc;
             k_ws_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->ws, E->scd + SD_TOI * ns, E->bscene, E->mass, P.ccd);
             E->launches++;
             E->has_ws = 0;
         }
         for (int it = 0; it < mi; it++) {
-            // contact.py:270-279 detection on the current iterate
+            // contact.py:270-279 detection on the current iterate: filter the
+            // swept list of the step that led here, or detect from scratch
             for (;;) {
                 int ph = phase_begin(E, PH_DETECT);
-                rc = eng_detect(E, P.cand_dist);
+                rc = E->sw_valid ? eng_detect_list(E) : eng_detect(E, P.cand_dist);
                 phase_end(E, ph, detect_bytes(E));
                 if (rc) return rc;
                 if ((rc = eng_sync_counters(E))) return rc;
@@ -143,19 +161,22 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             { int ph = phase_begin(E, PH_SOLVE); rc = eng_solve(E, &li); phase_end(E, ph, 0); if (rc) return rc; }
             st.lin_iters += li;
             st.n_active = E->hcnt->n_active;
-            // gauss_newton.py:98-115 line search
-            { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_masked(E, SD_E0, done); phase_end(E, ph, 0); if (rc) return rc; }
-            k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
-            E->launches++;
+            // candidates along x -> x - J du, shared by CCD, every energy
+            // of the line search and the next detection
+            { int ph = phase_begin(E, PH_DETECT); rc = eng_swept(E, E->du, -1.0, done); phase_end(E, ph, 0); if (rc) return rc; }
             if (P.ccd) {
-                int ph = phase_begin(E, PH_CCD); rc = eng_ccd(E, E->du, -1.0); phase_end(E, ph, 0);
+                int ph = phase_begin(E, PH_CCD); rc = eng_ccd_list(E, done); phase_end(E, ph, 0);
                 if (rc) return rc;
             }
+            // gauss_newton.py:98-115 line search
+            { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E0, done); phase_end(E, ph, 0); if (rc) return rc; }
+            k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
+            E->launches++;
             k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
             E->launches++;
             for (int trial = 0; trial < 64; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
-                { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_masked(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
+                { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
                 k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, P.ls_min_alpha, E->dcnt);
                 E->launches += 2;
                 st.ls_trials++;

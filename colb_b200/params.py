@@ -13,9 +13,14 @@ dhat = 2 * 0.0475 (barrier.py:4-5), candidate filter
 `config_params()` carries the synthetic-scene physics: triangle meshes
 with point-triangle + edge-edge + half-space contact, dhat = 1e-3,
 kappa = 1e7, k_ortho = 1e7, gravity (0,-9.8,0), CCD-bounded line search.
+Two choices differ from the reference constants because the stiff log
+barrier at dhat = 1e-3 needs them: the back-off line search keeps halving
+until the energy decreases (floor 1e-12 instead of accepting 1/64
+unconditionally, gauss_newton.py:110), and impacts take up to ~25 Newton
+iterations, so the cap is 64 (the residual target stays 1e-5).
 """
 from ._abi import (AbdParams, params_from_dict, params_to_dict, BARRIER_CUBIC, BARRIER_LOG,
-                   HESS_REFERENCE, HESS_PROJECTED, SOLVER_BICGSTAB, SOLVER_PCG, PREC_FP64)
+                   HESS_REFERENCE, HESS_PROJECTED, SOLVER_BICGSTAB, SOLVER_PCG, SOLVER_AUTO, PREC_FP64)
 
 REFERENCE = dict(
     dt=8e-3,
@@ -57,14 +62,14 @@ CONFIG = dict(
     contact_pt=1,
     self_contact=0,
     ee_f32=0,
-    linear_solver=SOLVER_PCG,
+    linear_solver=SOLVER_AUTO,
     lin_max_iter=2000,
     lin_tol=1e-6,
     newton_tol=1e-5,
-    newton_max_iter=16,
+    newton_max_iter=64,
     ccd=1,
     ccd_scale=0.1,
-    ls_min_alpha=1e-2,
+    ls_min_alpha=1e-12,
     precision=PREC_FP64,
     contact_capacity=1 << 20,
     pinned_diag=100.0,

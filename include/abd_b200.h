@@ -56,6 +56,10 @@ extern "C" {
 
 #define ABD_SOLVER_BICGSTAB    0   /* abd.py:636 uses bicgstab; here block-Jacobi preconditioned */
 #define ABD_SOLVER_PCG         1   /* block-Jacobi PCG */
+#define ABD_SOLVER_DIRECT      2   /* dense factorization per scene (the reference's solver_config="direct",
+                                      abd.py:637-654): Cholesky for projected Hessians, else LU */
+#define ABD_SOLVER_AUTO        3   /* DIRECT while the dense matrices fit (<= 64 scenes, <= 4 GiB), else PCG
+                                      (projected Hessian) or BiCGSTAB (reference Hessian) */
 
 #define ABD_PREC_FP64          0
 #define ABD_PREC_MIXED         1   /* FP32 block matrix + Krylov vectors; FP64 distances, CCD, energy, residual */
@@ -91,7 +95,10 @@ typedef struct AbdParams {
     int32_t precision;      /* ABD_PREC_* */
     int32_t contact_capacity;/* max candidate pairs per detection (reference: 10000, contact.py:8) */
     double pinned_diag;     /* diagonal of pinned bodies' blocks, abd.py:146 (100) */
-    int32_t warm_start;     /* 1: start Newton from nxt = now + user increment (abd_set_warm_start) */
+    int32_t warm_start;     /* 0: start Newton from nxt = now (abd.py: history.nxt == now after
+                               forward_states); 1: from now + the increment given to
+                               abd_set_warm_start; 2: from the inertial prediction
+                               (c + dt v + dt^2 g, q + dt qdot); 1 and 2 are clipped by CCD */
     int32_t reserved[7];
 } AbdParams;
 

@@ -1007,12 +1007,88 @@ done:
     return status;
 }
 
+/* Direct solve (abd.py:637-654 factors the assembled matrix): dense
+ * Cholesky when the Hessian is PSD-projected, else (or when a pivot is not
+ * positive) LU with partial pivoting. */
+static int dense_factor_solve(const AbdParams* P, const BSR* A, const double* b, double* x) {
+    int nb = A->nb; long n = 12L * nb;
+    double* M = (double*)calloc((size_t)(n * n), sizeof(double));
+    for (int r = 0; r < nb; r++) for (int k = A->rowptr[r]; k < A->rowptr[r+1]; k++) {
+        int c = A->col[k];
+        for (int i = 0; i < 12; i++) for (int j = 0; j < 12; j++)
+            M[(12L*r + i) * n + 12L*c + j] = A->val[144*k + 12*i + j];
+    }
+    memcpy(x, b, sizeof(double) * n);
+    int ok = 0;
+    if (P->hess_mode == ABD_HESS_PROJECTED) {
+        double* L = (double*)malloc(sizeof(double) * n * n);
+        memcpy(L, M, sizeof(double) * n * n);
+        ok = 1;
+        for (long j = 0; j < n && ok; j++) {
+            double d = L[j*n + j];
+            for (long k = 0; k < j; k++) d -= L[j*n + k] * L[j*n + k];
+            if (!(d > 0)) { ok = 0; break; }
+            d = sqrt(d); L[j*n + j] = d;
+            #pragma omp parallel for num_threads(g_threads) schedule(static)
+            for (long i = j + 1; i < n; i++) {
+                double v = L[i*n + j];
+                for (long k = 0; k < j; k++) v -= L[i*n + k] * L[j*n + k];
+                L[i*n + j] = v / d;
+            }
+        }
+        if (ok) {
+            for (long i = 0; i < n; i++) { double v = x[i]; for (long k = 0; k < i; k++) v -= L[i*n + k] * x[k]; x[i] = v / L[i*n + i]; }
+            for (long i = n - 1; i >= 0; i--) { double v = x[i]; for (long k = i + 1; k < n; k++) v -= L[k*n + i] * x[k]; x[i] = v / L[i*n + i]; }
+        }
+        free(L);
+        memcpy(x, ok ? x : b, sizeof(double) * n);
+        if (!ok) memcpy(x, b, sizeof(double) * n);
+    }
+    if (!ok) {
+        int* piv = (int*)malloc(sizeof(int) * n);
+        for (long j = 0; j < n; j++) {
+            long p = j; for (long i = j + 1; i < n; i++) if (fabs(M[i*n + j]) > fabs(M[p*n + j])) p = i;
+            piv[j] = (int)p;
+            if (p != j) { for (long k = 0; k < n; k++) { double t = M[j*n + k]; M[j*n + k] = M[p*n + k]; M[p*n + k] = t; }
+                          double t = x[j]; x[j] = x[p]; x[p] = t; }
+            double d = M[j*n + j];
+            if (d == 0.0) continue;
+            #pragma omp parallel for num_threads(g_threads) schedule(static)
+            for (long i = j + 1; i < n; i++) {
+                double f = M[i*n + j] / d;
+                M[i*n + j] = f;
+                if (f != 0.0) for (long k = j + 1; k < n; k++) M[i*n + k] -= f * M[j*n + k];
+            }
+            for (long i = j + 1; i < n; i++) x[i] -= M[i*n + j] * x[j];
+        }
+        for (long i = n - 1; i >= 0; i--) { double v = x[i]; for (long k = i + 1; k < n; k++) v -= M[i*n + k] * x[k]; x[i] = M[i*n + i] != 0 ? v / M[i*n + i] : 0; }
+        free(piv);
+    }
+    free(M);
+    return 0;
+}
+
+static int use_direct(const OracleWorld* w) {
+    int k = w->P.linear_solver;
+    if (k == 2) return 1;
+    if (k != 3) return 0;
+    long long tot = 0;
+    for (int i = 0; i < w->ns; i++) { long long n = 12LL * w->s[i].nb; tot += n * n; }
+    return w->ns <= 64 && tot * 8 <= (4LL << 30);
+}
+static int solve_system(const OracleWorld* w, const BSR* A, const double* b, double* x, int* iters) {
+    if (use_direct(w)) { *iters = 1; return dense_factor_solve(&w->P, A, b, x); }
+    AbdParams P = w->P;
+    if (P.linear_solver == 3) P.linear_solver = P.hess_mode == ABD_HESS_PROJECTED ? ABD_SOLVER_PCG : ABD_SOLVER_BICGSTAB;
+    return krylov(&P, A, b, x, iters);
+}
+
 int oracle_solve(OracleWorld* w, double* du, int* iters) {
     int tot = 0;
     for (int i = 0; i < w->ns; i++) {
         OScene* S = &w->s[i];
         Assembly as; assemble_scene(w, S, &as);
-        int it = 0; krylov(&w->P, &as.A, as.g, du, &it);
+        int it = 0; solve_system(w, &as.A, as.g, du, &it);
         tot += it; du += 12 * S->nb;
         free(as.g); bsr_free(&as.A);
     }
@@ -1132,6 +1208,15 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
     double* backup = (double*)xalloc(sizeof(double) * 48 * nb);
     double* du = (double*)xalloc(sizeof(double) * 12 * nb);
     double* pv = (double*)xalloc(sizeof(double) * 3 * S->nv);
+    if (P->warm_start == 2) {
+        /* inertial prediction as the initial increment */
+        for (int b = 0; b < nb; b++) {
+            const double* now = S->st + 48*b + ST_NOW;
+            for (int k = 0; k < 3; k++) S->ws[12*b + k] = dt * now[ST_V+k] + dt * dt * P->gravity[k];
+            for (int k = 0; k < 9; k++) S->ws[12*b + 3 + k] = dt * now[ST_QD+k];
+        }
+        S->has_ws = 1;
+    }
     if (S->has_ws) {
         memcpy(backup, S->st, sizeof(double) * 48 * nb);
         for (int i = 0; i < 12 * nb; i++) du[i] = -S->ws[i];
@@ -1146,7 +1231,7 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
     for (;;) {
         Assembly as; assemble_scene(w, S, &as);
         res = sqrt(vdot(12 * nb, as.g, as.g));
-        int li = 0; krylov(P, &as.A, as.g, du, &li);
+        int li = 0; solve_system(w, &as.A, as.g, du, &li);
         st->lin_iters += li; st->n_pairs = S->nc; st->n_active = as.n_active;
         free(as.g); bsr_free(&as.A);
         /* line search */
