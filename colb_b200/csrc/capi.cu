@@ -7,6 +7,7 @@
 #include <new>
 
 static std::string g_err;
+std::string& abd_global_error() { return g_err; }
 
 int eng_energy_masked(Engine* E, int slot, const int* skip);
 Geo eng_geo(Engine* E);

@@ -76,7 +76,7 @@ DV void grid_visit(const GridView& G, float4 qlo, float4 qhi, int scene, F&& vis
                 int e = G.bend[key];
                 for (int k = b; k < e; k++) {
                     int j = G.vals[k];
-                    if (G.scene[j] != scene) continue;
+                    if (G.scene && G.scene[j] != scene) continue;
                     float4 lo = G.lo[j];
                     if ((int)floorf(lo.x / h) != cx || (int)floorf(lo.y / h) != cy || (int)floorf(lo.z / h) != cz) continue;
                     float4 hi = G.hi[j];

@@ -21,6 +21,7 @@ EXPORTS = [
     "abd_step", "abd_get_profile", "abd_get_vertices", "abd_get_pairs", "abd_get_contact_points",
     "abd_energy", "abd_assemble", "abd_solve", "abd_set_warm_start", "abd_get_features",
     "abd_count_intersections", "abd_last_error", "abd_abi_version", "abd_set_timing", "abd_get_timing",
+    "abd_ee_pairs_static",
 ]
 PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv"]
 
@@ -63,6 +64,7 @@ def load_library(path=LIB_PATH):
     L.abd_abi_version.argtypes = []
     L.abd_set_timing.argtypes = [vp, C.c_int32, C.c_int32]
     L.abd_get_timing.argtypes = [vp, dp, C.POINTER(C.c_int64), dp]
+    L.abd_ee_pairs_static.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_double, vp, C.c_int32, vp, vp]
     _lib = L
     return L
 

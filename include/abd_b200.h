@@ -232,6 +232,28 @@ int abd_count_intersections(AbdHandle* h, int32_t* count);
 int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset);
 int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes);
 
+/* Edge-edge candidate pairs that allocate no device memory.  This entry
+ * point has no counterpart in the reference; it exists for callers that
+ * cannot call cudaMalloc when they need the pairs (a host that manages all
+ * device memory through its own pool, a real-time loop that forbids
+ * allocation after start-up, a plugin whose host owns the CUDA context).
+ * It computes the same sorted set as abd_get_pairs for an EE-only scene
+ * under the reference predicate (contact.py:158-168: i < j, no shared
+ * vertex, float32 segment distance < cand_dist), written as vertex
+ * quadruples (a1, a2, b1, b2), but takes DEVICE pointers: x_dev (n_verts*3
+ * doubles), edges_dev (n_edges*2 ints), pairs_dev (cap*4 ints) and
+ * n_pairs_dev (one int).  All scratch lives in static device arrays of the
+ * library sized for ABD_STATIC_MAX_EDGES edges; larger inputs are rejected
+ * with ABD_ERR_INVALID_ARG.  The first call on each device looks those
+ * arrays up (make it before any stream capture).  Calls share the arrays:
+ * calls whose GPU work overlaps race.  Work runs on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) and the call returns
+ * after synchronising it; ABD_ERR_CONTACT_OVERFLOW if more than cap pairs
+ * exist (*n_pairs_dev holds the full count).  Errors: abd_last_error(NULL). */
+#define ABD_STATIC_MAX_EDGES (1 << 16)
+int abd_ee_pairs_static(const double* x_dev, const int32_t* edges_dev, int32_t n_verts, int32_t n_edges,
+                        double cand_dist, int32_t* pairs_dev, int32_t cap, int32_t* n_pairs_dev, void* stream);
+
 /* Message of the last failing call on this handle (or a global one for NULL). */
 const char* abd_last_error(AbdHandle* h);
 
