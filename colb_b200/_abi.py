@@ -53,7 +53,8 @@ class AbdParams(C.Structure):
         ("contact_capacity", C.c_int32),
         ("pinned_diag", C.c_double),
         ("warm_start", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("broadphase", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

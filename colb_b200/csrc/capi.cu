@@ -88,6 +88,10 @@ int eng_grow_contacts(Engine* E, int need) {
     return ABD_OK;
 }
 
+bool eng_use_bp(const Engine* E) {
+    return E->bd_ok && (E->P.broadphase == 2 || E->P.broadphase == 0);
+}
+
 int eng_grow_swept(Engine* E, int need) {
     int cap = std::max(need + need / 4 + 1024, 2 * E->sw_cap);
     cudaStreamSynchronize(E->stream);
@@ -138,6 +142,9 @@ int eng_alloc(Engine* E) {
 
 void eng_free(Engine* E) {
     eng_dense_free(E);
+    eng_bp_free(E);
+    void* bd[] = {E->bd_vbeg, E->bd_ebeg, E->bd_tbeg};
+    for (void* p : bd) if (p) cudaFree(p);
     grid_free(E->gee); grid_free(E->gpt);
     void* ps[] = {E->xbar, E->vbody, E->vscene, E->bscene, E->edges, E->tris, E->mass, E->J, E->planes, E->plane_scene,
                   E->sc_plane_begin, E->sc_body_begin, E->edge_scene, E->tri_scene, E->st, E->backup, E->du, E->g, E->x,
@@ -248,6 +255,7 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     E->h_body_begin = sc_body_begin;
     E->h_edges = edges; E->h_tris = tris;
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) { delete E; g_err = "stream"; return ABD_ERR_CUDA; }
+    if (P.broadphase < 0 || P.broadphase > 2) { delete E; g_err = "abd_create: broadphase must be 0, 1 or 2"; return ABD_ERR_INVALID_ARG; }
     auto up = [&](auto*& dst, auto& src) -> int {
         using T = typename std::remove_reference<decltype(src)>::type::value_type;
         int rc = dalloc(E, (T**)&dst, src.size());
@@ -267,6 +275,33 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
         g_err = E->err; eng_free(E); delete E; return rc;
     }
     E->edges = reinterpret_cast<int2*>(edges_i);
+    // per-body primitive ranges for the body-pair broad phase
+    {
+        std::vector<int> vb(nb + 1, 0), eb(nb + 1, 0), tb(nb + 1, 0);
+        bool ok = true;
+        auto ranges = [&](const std::vector<int>& owner, std::vector<int>& beg) {
+            int cur = 0; beg[0] = 0;
+            for (size_t i = 0; i < owner.size(); i++) {
+                int b = owner[i];
+                if (b < cur) { ok = false; return; }
+                while (cur < b) { beg[++cur] = (int)i; }
+            }
+            while (cur < nb) beg[++cur] = (int)owner.size();
+        };
+        std::vector<int> eown(E->ne), town(E->nt);
+        for (int e = 0; e < E->ne; e++) eown[e] = vbody[edges[2*e]];
+        for (int t = 0; t < E->nt; t++) {
+            int b0 = vbody[tris[3*t]];
+            if (vbody[tris[3*t+1]] != b0 || vbody[tris[3*t+2]] != b0) ok = false;
+            town[t] = b0;
+        }
+        for (int e = 0; e < E->ne; e++) if (vbody[edges[2*e+1]] != eown[e]) ok = false;
+        ranges(vbody, vb); ranges(eown, eb); ranges(town, tb);
+        E->bd_ok = ok;
+        if (ok && ((rc = up(E->bd_vbeg, vb)) || (rc = up(E->bd_ebeg, eb)) || (rc = up(E->bd_tbeg, tb)))) {
+            g_err = E->err; eng_free(E); delete E; return rc;
+        }
+    }
     if (cudaMemcpy(E->st, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
         g_err = "cudaMemcpy state"; eng_free(E); delete E; return ABD_ERR_CUDA;
     }
@@ -343,7 +378,7 @@ int abd_get_vertices(AbdHandle* h, double* x) {
 static int detect_full(Engine* E) {
     int rc;
     for (;;) {
-        if ((rc = eng_detect(E, E->P.cand_dist))) return rc;
+        if ((rc = eng_use_bp(E) ? eng_detect_bp(E, E->P.cand_dist) : eng_detect(E, E->P.cand_dist))) return rc;
         if ((rc = eng_sync_counters(E))) return rc;
         if (!E->hcnt->overflow) return ABD_OK;
         if ((rc = eng_grow_contacts(E, E->hcnt->n_total))) return rc;

@@ -160,6 +160,9 @@ struct Engine {
 
     double* prof_d = nullptr;      // [2][ns][newton_max_iter] residual / alpha of the current step
     void* dense_state = nullptr;   // direct-solver state (dense.cu)
+    void* bp_state = nullptr;      // body-pair broad phase scratch (bpair.cu)
+    bool bd_ok = false;            // bodies own contiguous vertex / edge / triangle ranges
+    int* bd_vbeg = nullptr; int* bd_ebeg = nullptr; int* bd_tbeg = nullptr;   // [nb+1]
     int krylov_kind = ABD_SOLVER_BICGSTAB;
     std::vector<int> h_edges, h_tris;  // host copies (global vertex ids) for abd_get_pairs
 
@@ -230,3 +233,7 @@ int eng_swept(Engine* E, const double* dq, double sign, const int* done);
 int eng_ccd_list(Engine* E, const int* skip);
 int eng_energy_list(Engine* E, int slot, const int* skip);
 int eng_detect_list(Engine* E);
+int eng_swept_bp(Engine* E, double lim);
+int eng_detect_bp(Engine* E, double filt);
+void eng_bp_free(Engine* E);
+bool eng_use_bp(const Engine* E);

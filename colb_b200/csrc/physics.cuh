@@ -318,14 +318,15 @@ DV void psd_project(int n, double* H) {
     for (int i = 0; i < n * n; i++) { A[i] = H[i]; fro += H[i] * H[i]; }
     if (fro == 0.0) return;
     for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) V[i*n+j] = (i == j) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 100; sweep++) {
-        double off = 0;
-        for (int p = 0; p < n; p++) for (int q = p + 1; q < n; q++) off += A[p*n+q] * A[p*n+q];
-        if (off <= 1e-32 * fro) break;
+    // a rotation is skipped when |a_pq| is at rounding level against the
+    // diagonal; the sweeps stop when none was applied (scale-invariant)
+    for (int sweep = 0; sweep < 50; sweep++) {
+        int rotated = 0;
         for (int p = 0; p < n; p++)
             for (int q = p + 1; q < n; q++) {
                 double apq = A[p*n+q];
-                if (apq == 0.0) continue;
+                if (fabs(apq) <= 1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])) + 1e-300 * fro) continue;
+                rotated = 1;
                 double theta = (A[q*n+q] - A[p*n+p]) / (2 * apq);
                 double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
                 double c = rsqrt(t * t + 1), s = t * c;
@@ -342,6 +343,7 @@ DV void psd_project(int n, double* H) {
                     V[k*n+p] = c * vkp - s * vkq; V[k*n+q] = s * vkp + c * vkq;
                 }
             }
+        if (!rotated) break;
     }
     for (int i = 0; i < n; i++)
         for (int j = 0; j < n; j++) {

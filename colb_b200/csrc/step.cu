@@ -146,7 +146,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             // swept list of the step that led here, or detect from scratch
             for (;;) {
                 int ph = phase_begin(E, PH_DETECT);
-                rc = E->sw_valid ? eng_detect_list(E) : eng_detect(E, P.cand_dist);
+                rc = E->sw_valid ? eng_detect_list(E) : (eng_use_bp(E) ? eng_detect_bp(E, P.cand_dist) : eng_detect(E, P.cand_dist));
                 phase_end(E, ph, detect_bytes(E));
                 if (rc) return rc;
                 if ((rc = eng_sync_counters(E))) return rc;

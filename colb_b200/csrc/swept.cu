@@ -186,6 +186,13 @@ int eng_swept(Engine* E, const double* dq, double sign, const int* done) {
     int rc;
     double lim = P.cand_dist * (1.0 + 1e-6) + 1e-7;
     float pad = (float)(0.5 * lim);
+    if (eng_use_bp(E)) {
+        if ((rc = eng_transform(E))) return rc;
+        k_vertex_disp2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, E->vbody, E->xbar, dq, sign, E->mass, E->bscene, done,
+                                                        E->pv, E->pmag);
+        E->launches++;
+        return eng_swept_bp(E, lim);
+    }
     for (;;) {
         if ((rc = eng_transform(E))) return rc;
         k_vertex_disp2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, E->vbody, E->xbar, dq, sign, E->mass, E->bscene, done,

@@ -99,7 +99,9 @@ typedef struct AbdParams {
                                forward_states); 1: from now + the increment given to
                                abd_set_warm_start; 2: from the inertial prediction
                                (c + dt v + dt^2 g, q + dt qdot); 1 and 2 are clipped by CCD */
-    int32_t reserved[7];
+    int32_t broadphase;     /* 0 auto, 1 hashed grid over primitives, 2 body pairs then primitives
+                               (needs contiguous per-body vertex/edge/triangle ranges) */
+    int32_t reserved[6];
 } AbdParams;
 
 /* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */

@@ -31,8 +31,9 @@ def test_transform_bitexact(chain_scene, chain_pairs):
         assert np.array_equal(e.vertices(), o.vertices())
 
 
-def test_chain_pairs_bitexact_vs_golden(chain_scene, chain_pairs):
-    e = Engine(P.reference_params(), chain_scene)
+@pytest.mark.parametrize("broadphase", [1, 2])
+def test_chain_pairs_bitexact_vs_golden(chain_scene, chain_pairs, broadphase):
+    e = Engine(P.reference_params(broadphase=broadphase), chain_scene)
     for k in range(3):
         e.set_state(chain_pairs["states"][k])
         quads, kinds = e.pairs()
@@ -40,10 +41,11 @@ def test_chain_pairs_bitexact_vs_golden(chain_scene, chain_pairs):
         assert np.array_equal(_edge_pairs(chain_scene, quads), chain_pairs[f"pairs{k}"])
 
 
+@pytest.mark.parametrize("broadphase", [1, 2])
 @pytest.mark.parametrize("which", ["cubes", "net"])
-def test_config_pairs_match_oracle(which):
+def test_config_pairs_match_oracle(which, broadphase):
     sc = S.config1_cubes(seed=3) if which == "cubes" else S.config2_chain_net(n=3, seed=1)
-    p = P.config_params(cand_dist=0.05)
+    p = P.config_params(cand_dist=0.05, broadphase=broadphase)
     e, o = _pair(p, sc)
     st = sc["state"].copy()
     rng = np.random.default_rng(5)
@@ -97,8 +99,9 @@ def test_solve_matches_dense(chain_scene, chain_pairs, solver):
     assert it > 0
 
 
-def test_reference_chain_trajectory(chain_scene):
-    p = P.reference_params(lin_tol=1e-10)
+@pytest.mark.parametrize("broadphase", [1, 2])
+def test_reference_chain_trajectory(chain_scene, broadphase):
+    p = P.reference_params(lin_tol=1e-10, broadphase=broadphase)
     e, o = _pair(p, chain_scene)
     for _ in range(4):
         rc, se = e.step(5)
@@ -109,9 +112,10 @@ def test_reference_chain_trajectory(chain_scene):
     assert se.unconverged == 0
 
 
-def test_config_cubes_trajectory_and_no_intersection():
+@pytest.mark.parametrize("broadphase", [1, 2])
+def test_config_cubes_trajectory_and_no_intersection(broadphase):
     sc = S.config1_cubes(seed=0)
-    p = P.config_params(lin_tol=1e-10)
+    p = P.config_params(lin_tol=1e-10, broadphase=broadphase)
     e, o = _pair(p, sc)
     for _ in range(3):
         e.step(10); o.step(10)
@@ -143,8 +147,9 @@ def test_mixed_precision_close_to_fp64(chain_scene):
     assert np.abs(x64 - x32).max() <= 1e-4 * np.abs(x64).max()
 
 
-def test_contact_capacity_grows(chain_scene, chain_pairs):
-    e = Engine(P.reference_params(contact_capacity=64), chain_scene)
+@pytest.mark.parametrize("broadphase", [1, 2])
+def test_contact_capacity_grows(chain_scene, chain_pairs, broadphase):
+    e = Engine(P.reference_params(contact_capacity=64, broadphase=broadphase), chain_scene)
     e.set_state(chain_pairs["states"][2])
     quads, _ = e.pairs()
     assert np.array_equal(_edge_pairs(chain_scene, quads), chain_pairs["pairs2"])
@@ -162,3 +167,19 @@ def test_invalid_arguments_return_errors(chain_scene):
         e.set_warm_start(np.zeros((e.nb, 12)))  # features path is fine; warm start of the wrong size below
         e.L  # noqa: B018
         raise AbdError(-1, "sentinel")
+
+
+def test_net_trajectory_matches_oracle():
+    """3x3 chain mail with contacts from the first step (pitch just under
+    the touching distance): PT + EE contacts, log barrier, direct solve,
+    CCD, monotone line search."""
+    sc = S.config2_chain_net(n=3, pitch=1.5 - 5e-4, seed=2)
+    p = P.config_params(dt=1.0 / 240.0, linear_solver=2)
+    e, o = _pair(p, sc)
+    for _ in range(3):
+        rc, se = e.step(2)
+        o.step(2)
+        xe, xo = e.vertices(), o.vertices()
+        assert np.abs(xe - xo).max() <= 1e-6 * np.abs(xo).max()
+    assert se.n_active > 0
+    assert e.count_intersections() == 0
