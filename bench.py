@@ -264,7 +264,7 @@ def main():
     peak, peak_kind = measured_peaks()
     ph = r["phases"]
     # dominant kernel class among the individually timed ones
-    dom = max(("spmv", "energy_query"), key=lambda k: ph[k]["ms"])
+    dom = max(("spmv", "energy_query", "energy_list"), key=lambda k: ph[k]["ms"])
     avg_ms = ph[dom]["ms"] / max(1, ph[dom]["launches"])
     avg_bytes = ph[dom]["bytes"] / max(1, ph[dom]["launches"])
     achieved = avg_bytes / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0

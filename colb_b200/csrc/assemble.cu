@@ -15,9 +15,11 @@
 // contact adds its four body blocks into that structure with FP64/FP32
 // atomics.
 #include "contact.cuh"
+#include "warp_eig.cuh"
 #include <cub/cub.cuh>
 
 Geo eng_geo(Engine* E);
+bool eng_solver_is_direct(const Engine* E);
 
 DV int stencil_np(int type) { return type == T_PP ? 2 : (type == T_PE ? 3 : (type == T_PG ? 1 : 4)); }
 DV int other_vertex(int type, int4 s) { return type == T_EE ? s.z : (type == T_PG ? s.x : s.y); }
@@ -80,135 +82,295 @@ __global__ void k_zero_vals(const Counters* cnt, T* vals) {
 }
 
 // ---------------------------------------------------- inertia + ortho (abd.py:108-149)
+// One warp per body: gradient by lanes 0..11, the 9x9 orthogonality Hessian
+// (scaled by dt^2) built lane-parallel in shared memory, projected to PSD
+// when requested, and written with the mass terms into the diagonal block.
+#define BA_WARPS 4
 template <class T>
-__global__ void k_body_assemble(int nb, const double* __restrict__ st, const double* __restrict__ mass,
-                                const double* __restrict__ J, double dt, double g0, double g1, double g2,
-                                double k_ortho, int project, double pinned_diag, const int* __restrict__ row_ptr,
-                                const int* __restrict__ bcol, T* vals, double* grad) {
-    GS_LOOP(b, nb) {
-        int bi = find_block(row_ptr, bcol, (int)b, (int)b);
-        if (bi < 0) continue;                 // every row holds its diagonal key
+__global__ void __launch_bounds__(32 * BA_WARPS) k_body_assemble(int nb, const double* __restrict__ st,
+                                const double* __restrict__ mass, const double* __restrict__ J, double dt, double g0,
+                                double g1, double g2, double k_ortho, int project, double pinned_diag,
+                                const int* __restrict__ row_ptr, const int* __restrict__ bcol, T* vals, double* grad) {
+    __shared__ WarpEigSmem sm[BA_WARPS];
+    __shared__ double sq[BA_WARPS][9];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpEigSmem& E = sm[w];
+    for (int b = blockIdx.x * BA_WARPS + w; b < nb; b += gridDim.x * BA_WARPS) {
+        int bi = find_block(row_ptr, bcol, b, b);
+        if (bi < 0) continue;                              // every row holds its diagonal key
         T* V = vals + (long)bi * 144;
-        double* g = grad + 12 * b;
+        double* g = grad + 12L * b;
         double m = mass[b];
-        if (m > 0.0) {
-            const double* now = st + ST_STRIDE * b + ST_NOW; const double* nx = st + ST_STRIDE * b + ST_NXT;
-            double q[9];
-#pragma unroll
-            for (int i = 0; i < 9; i++) q[i] = nx[ST_Q + i];
-            double go[9]; ortho_grad(q, k_ortho, go);
-            double gv[3] = {g0, g1, g2};
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                double ct = now[ST_C+k] + dt * now[ST_V+k] + dt * dt * gv[k];
-                g[k] = (nx[ST_C+k] - ct) * m;
-            }
-            double Jb = J[b];
-#pragma unroll
-            for (int r = 0; r < 9; r++) {
-                double qt = now[ST_Q+r] + dt * now[ST_QD+r];
-                g[3+r] = dt * dt * go[r] + (q[r] - qt) * Jb;
-            }
-            double H[81];
-            for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++)
-                for (int r = 0; r < 3; r++) for (int c = 0; c < 3; c++)
-                    H[(3*i+r)*9 + 3*j+c] = ortho_hess(q, k_ortho, i, j, r, c) * dt * dt;
-            if (project) psd_project(9, H);
-            for (int c = 0; c < 12; c++)
-                for (int r = 0; r < 12; r++) {
-                    double v;
-                    if (r < 3 || c < 3) v = (r == c) ? m : 0.0;
-                    else v = H[(r-3)*9 + (c-3)] + (r == c ? Jb : 0.0);
-                    V[c*12 + r] = (T)v;
-                }
-        } else {
-            for (int k = 0; k < 12; k++) g[k] = 0.0;
-            for (int c = 0; c < 12; c++) for (int r = 0; r < 12; r++) V[c*12 + r] = (T)(r == c ? pinned_diag : 0.0);
+        if (!(m > 0.0)) {
+            if (lane < 12) g[lane] = 0.0;
+            for (int e = lane; e < 144; e += 32) V[e] = (T)((e % 12 == e / 12) ? pinned_diag : 0.0);
+            continue;
         }
+        const double* now = st + ST_STRIDE * (long)b + ST_NOW; const double* nx = st + ST_STRIDE * (long)b + ST_NXT;
+        if (lane < 9) sq[w][lane] = nx[ST_Q + lane];
+        __syncwarp();
+        const double* q = sq[w];
+        double Jb = J[b];
+        if (lane < 3) {
+            double gv = lane == 0 ? g0 : (lane == 1 ? g1 : g2);
+            double ct = now[ST_C + lane] + dt * now[ST_V + lane] + dt * dt * gv;
+            g[lane] = (nx[ST_C + lane] - ct) * m;
+        } else if (lane < 12) {
+            int r = lane - 3, i = r / 3, c = r % 3;
+            double gi = -q[3*i+c];
+            for (int j = 0; j < 3; j++) gi += (q[3*i]*q[3*j] + q[3*i+1]*q[3*j+1] + q[3*i+2]*q[3*j+2]) * q[3*j+c];
+            double qt = now[ST_Q + r] + dt * now[ST_QD + r];
+            g[lane] = dt * dt * (gi * 4.0 * k_ortho) + (q[r] - qt) * Jb;
+        }
+        for (int e = lane; e < 81; e += 32) {
+            int rr = e / 9, cc = e % 9;
+            E.A[rr*12 + cc] = ortho_hess(q, k_ortho, rr / 3, cc / 3, rr % 3, cc % 3) * dt * dt;
+        }
+        __syncwarp();
+        if (project) warp_psd_project(E, 9);
+        for (int e = lane; e < 144; e += 32) {
+            int row = e % 12, col = e / 12;
+            double v;
+            if (row < 3 || col < 3) v = (row == col) ? m : 0.0;
+            else v = E.A[(row-3)*12 + (col-3)] + (row == col ? Jb : 0.0);
+            V[e] = (T)v;
+        }
+        __syncwarp();
     }
 }
 
 // ---------------------------------------------------- contacts (abd.py:198-571)
+// One warp per active contact.  The stencil's squared-distance gradient and
+// Hessian are built lane-parallel in shared memory (auxiliary vectors by
+// lane 0, matrix entries by all lanes), chained through the barrier,
+// projected to PSD by the warp Jacobi (warp_eig.cuh), and scattered into the
+// body blocks: lanes own block entries, each summing the stencil vertices
+// that map to it through J = [1, xbar^T] (x) I3.
+#define CA_WARPS 4
+struct ContactSmem {
+    WarpEigSmem E;
+    double x[12], g[12], gy[9], aux[48], J[4][4];
+    double B0, B1, B2;
+    int v[4], vb[4], np, type, bodies[2], nbd;
+};
+
+// C[point][aux] maps for the (w, u, v) and (w, e) parameterisations
+__constant__ signed char c_map_ee[4][3] = {{1, -1, 0}, {0, 1, 0}, {-1, 0, -1}, {0, 0, 1}};
+__constant__ signed char c_map_pt[4][3] = {{1, 0, 0}, {-1, -1, -1}, {0, 1, 0}, {0, 0, 1}};
+__constant__ signed char c_map_pe[3][2] = {{1, 0}, {-1, -1}, {0, 1}};
+
+DV void skew9(const double* a, double* S) {
+    S[0] = 0; S[1] = -a[2]; S[2] = a[1]; S[3] = a[2]; S[4] = 0; S[5] = -a[0]; S[6] = -a[1]; S[7] = a[0]; S[8] = 0;
+}
+DV void cross3(const double* a, const double* b, double* o) {
+    o[0] = a[1]*b[2] - a[2]*b[1]; o[1] = a[2]*b[0] - a[0]*b[2]; o[2] = a[0]*b[1] - a[1]*b[0];
+}
+
+// squared distance gradient (C.g) and Hessian (C.E.A, ld 12) of the stencil
+DV void warp_distance_derivs(ContactSmem& C, const Geo& G) {
+    const int lane = threadIdx.x & 31;
+    const int m = 3 * C.np;
+    double* A = C.E.A; double* Hy = C.E.T;
+    if (C.type == T_PG) {
+        if (lane == 0) {
+            const double* nn = G.planes + 4 * C.v[1];
+            double d = nn[0] * C.x[0] + nn[1] * C.x[1] + nn[2] * C.x[2] - nn[3];
+            for (int k = 0; k < 3; k++) { C.g[k] = 2 * d * nn[k]; C.aux[k] = nn[k]; }
+        }
+        __syncwarp();
+        if (lane < 9) A[(lane / 3) * 12 + lane % 3] = 2 * C.aux[lane / 3] * C.aux[lane % 3];
+    } else if (C.type == T_PP) {
+        if (lane < 6) { int k = lane % 3; double d = C.x[k] - C.x[3 + k]; C.g[lane] = lane < 3 ? 2 * d : -2 * d; }
+        for (int e = lane; e < 36; e += 32) {
+            int i = e / 6, j = e % 6;
+            A[i*12+j] = (i % 3 == j % 3) ? ((i < 3) == (j < 3) ? 2.0 : -2.0) : 0.0;
+        }
+    } else if (C.type == T_PE) {
+        // w = p - e0, e = e1 - e0, f = w.w - (w.e)^2/(e.e)
+        if (lane == 0) {
+            double w[3], e[3];
+            for (int k = 0; k < 3; k++) { w[k] = C.x[k] - C.x[3+k]; e[k] = C.x[6+k] - C.x[3+k]; }
+            double c = w[0]*e[0] + w[1]*e[1] + w[2]*e[2], s2 = e[0]*e[0] + e[1]*e[1] + e[2]*e[2], is = 1.0 / s2;
+            for (int k = 0; k < 3; k++) {
+                C.aux[k] = w[k]; C.aux[3+k] = e[k];
+                C.gy[k] = 2*w[k] - 2*c*is*e[k];
+                C.gy[3+k] = -2*c*is*w[k] + 2*c*c*is*is*e[k];
+            }
+            C.aux[6] = c; C.aux[7] = is;
+        }
+        __syncwarp();
+        const double* W = C.aux; const double* Ev = C.aux + 3;
+        double c = C.aux[6], is = C.aux[7];
+        for (int e = lane; e < 36; e += 32) {
+            int i = e / 6, j = e % 6, bi = i / 3, bj = j / 3, r = i % 3, q = j % 3;
+            double I = (r == q) ? 1.0 : 0.0, h;
+            if (bi == 0 && bj == 0) h = 2*I - 2*is*Ev[r]*Ev[q];
+            else if (bi == 0 && bj == 1) h = -2*is*Ev[r]*W[q] - 2*c*is*I + 4*c*is*is*Ev[r]*Ev[q];
+            else if (bi == 1 && bj == 0) h = -2*is*Ev[q]*W[r] - 2*c*is*I + 4*c*is*is*Ev[q]*Ev[r];
+            else h = -2*is*W[r]*W[q] + 4*c*is*is*(W[r]*Ev[q] + Ev[r]*W[q]) - 8*c*c*is*is*is*Ev[r]*Ev[q] + 2*c*c*is*is*I;
+            Hy[i*6+j] = h;
+        }
+        __syncwarp();
+        if (lane < 9) {
+            int pnt = lane / 3, k = lane % 3;
+            C.g[lane] = c_map_pe[pnt][0] * C.gy[k] + c_map_pe[pnt][1] * C.gy[3+k];
+        }
+        for (int e = lane; e < 81; e += 32) {
+            int i = e / 9, j = e % 9, pi = i / 3, pj = j / 3, r = i % 3, q = j % 3;
+            double acc = 0;
+            for (int a = 0; a < 2; a++) if (c_map_pe[pi][a])
+                for (int b = 0; b < 2; b++) if (c_map_pe[pj][b])
+                    acc += c_map_pe[pi][a] * c_map_pe[pj][b] * Hy[(3*a+r)*6 + 3*b+q];
+            A[i*12+j] = acc;
+        }
+    } else {
+        // f = (w.n)^2/(n.n), n = u x v; EE: w = a0-b0, u = a1-a0, v = b1-b0;
+        // PT: w = p-t0, u = t1-t0, v = t2-t0
+        if (lane == 0) {
+            double w[3], u[3], v[3];
+            for (int k = 0; k < 3; k++) {
+                if (C.type == T_EE) { w[k] = C.x[k] - C.x[6+k]; u[k] = C.x[3+k] - C.x[k]; v[k] = C.x[9+k] - C.x[6+k]; }
+                else { w[k] = C.x[k] - C.x[3+k]; u[k] = C.x[6+k] - C.x[3+k]; v[k] = C.x[9+k] - C.x[3+k]; }
+            }
+            double n[3]; cross3(u, v, n);
+            double a = w[0]*n[0] + w[1]*n[1] + w[2]*n[2], b = n[0]*n[0] + n[1]*n[1] + n[2]*n[2], ib = 1.0 / b;
+            double vw[3], wu[3], vn[3], nu[3];
+            cross3(v, w, vw); cross3(w, u, wu); cross3(v, n, vn); cross3(n, u, nu);
+            double* ga = C.aux; double* gb = C.aux + 9;
+            for (int k = 0; k < 3; k++) {
+                ga[k] = n[k]; ga[3+k] = vw[k]; ga[6+k] = wu[k];
+                gb[k] = 0; gb[3+k] = 2*vn[k]; gb[6+k] = 2*nu[k];
+            }
+            skew9(u, C.aux + 18); skew9(v, C.aux + 27); skew9(w, C.aux + 36);
+            double Sn[9]; skew9(n, Sn);
+            // Sn is needed only in the (u,v) blocks: keep it in gy's slot after gy is consumed
+            for (int i = 0; i < 9; i++) C.gy[i] = 2*a*ib*ga[i] - a*a*ib*ib*gb[i];
+            C.aux[45] = a; C.aux[46] = ib;
+            for (int i = 0; i < 9; i++) C.E.V[i] = Sn[i];          // V is free until the projection
+        }
+        __syncwarp();
+        const double* ga = C.aux; const double* gb = C.aux + 9;
+        const double* Su = C.aux + 18; const double* Sv = C.aux + 27; const double* Sw = C.aux + 36;
+        const double* Sn = C.E.V;
+        double a = C.aux[45], ib = C.aux[46];
+        double c1 = 2*ib, c2 = 2*a*ib, c3 = 2*a*ib*ib, c4 = 2*a*a*ib*ib*ib, c5 = a*a*ib*ib;
+        for (int e = lane; e < 81; e += 32) {
+            int i = e / 9, j = e % 9, bi = i / 3, bj = j / 3, r = i % 3, c = j % 3;
+            double ha = 0, hb = 0;
+            if (bi == 0 && bj == 1) ha = -Sv[3*r+c];
+            else if (bi == 1 && bj == 0) ha = -Sv[3*c+r];
+            else if (bi == 0 && bj == 2) ha = Su[3*r+c];
+            else if (bi == 2 && bj == 0) ha = Su[3*c+r];
+            else if (bi == 1 && bj == 2) ha = -Sw[3*r+c];
+            else if (bi == 2 && bj == 1) ha = -Sw[3*c+r];
+            if (bi == 1 && bj == 1) { double t = 0; for (int q = 0; q < 3; q++) t += Sv[3*q+r] * Sv[3*q+c]; hb = 2*t; }
+            else if (bi == 1 && bj == 2) { double t = 0; for (int q = 0; q < 3; q++) t += Sv[3*r+q] * Su[3*q+c]; hb = 2*t - 2*Sn[3*r+c]; }
+            else if (bi == 2 && bj == 1) { double t = 0; for (int q = 0; q < 3; q++) t += Su[3*r+q] * Sv[3*q+c]; hb = 2*t + 2*Sn[3*r+c]; }
+            else if (bi == 2 && bj == 2) { double t = 0; for (int q = 0; q < 3; q++) t += Su[3*q+r] * Su[3*q+c]; hb = 2*t; }
+            Hy[i*9+j] = c1*ga[i]*ga[j] + c2*ha - c3*(ga[i]*gb[j] + gb[i]*ga[j]) + c4*gb[i]*gb[j] - c5*hb;
+        }
+        __syncwarp();
+        const signed char (*Cm)[3] = C.type == T_EE ? c_map_ee : c_map_pt;
+        if (lane < 12) {
+            int pnt = lane / 3, k = lane % 3;
+            double acc = 0;
+            for (int q = 0; q < 3; q++) acc += Cm[pnt][q] * C.gy[3*q+k];
+            C.g[lane] = acc;
+        }
+        for (int e = lane; e < 144; e += 32) {
+            int i = e / 12, j = e % 12, pi = i / 3, pj = j / 3, r = i % 3, q = j % 3;
+            double acc = 0;
+            for (int aa = 0; aa < 3; aa++) if (Cm[pi][aa])
+                for (int bb = 0; bb < 3; bb++) if (Cm[pj][bb])
+                    acc += Cm[pi][aa] * Cm[pj][bb] * Hy[(3*aa+r)*9 + 3*bb+q];
+            A[i*12+j] = acc;
+        }
+    }
+    (void)m;
+    __syncwarp();
+}
+
 template <class T>
-__global__ void k_contact_assemble(const Counters* cnt, const int4* __restrict__ cst, const int* __restrict__ ctype,
-                                   const double* __restrict__ cxb, Geo G, int barrier, double dhat, double sc,
-                                   int hess_mode, const int* __restrict__ row_ptr, const int* __restrict__ bcol,
-                                   T* vals, double* grad) {
-    int n = cnt->n_total;
-    GS_LOOP(c, n) {
+__global__ void __launch_bounds__(32 * CA_WARPS) k_contact_assemble(const Counters* cnt, const int4* __restrict__ cst,
+                                   const int* __restrict__ ctype, const double* __restrict__ cxb, Geo G, int barrier,
+                                   double dhat, double sc, int hess_mode, const int* __restrict__ row_ptr,
+                                   const int* __restrict__ bcol, T* vals, double* grad) {
+    __shared__ ContactSmem sm[CA_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    ContactSmem& C = sm[w];
+    const int n = cnt->n_total;
+    for (int c = blockIdx.x * CA_WARPS + w; c < n; c += gridDim.x * CA_WARPS) {
         int type = ctype[c];
-        if (type < 0) continue;
-        int4 s4 = cst[c];
-        int sv[4] = {s4.x, s4.y, s4.z, s4.w};
-        int np = stencil_np(type);
-        int m = 3 * np;
-        double g[12], H[144];
-        if (type == T_PG) {
-            const double* nrm = G.planes + 4 * s4.y;
-            double d = nrm[0] * G.x[3*s4.x] + nrm[1] * G.x[3*s4.x+1] + nrm[2] * G.x[3*s4.x+2] - nrm[3];
-            for (int r = 0; r < 3; r++) { g[r] = 2 * d * nrm[r]; for (int q = 0; q < 3; q++) H[r*3+q] = 2 * nrm[r] * nrm[q]; }
-            sv[1] = -1;
-        } else if (type == T_PP) {
-            d2_pp_full(ld3(G.x + 3*sv[0]), ld3(G.x + 3*sv[1]), g, H);
-        } else if (type == T_PE) {
-            d2_pe_full(ld3(G.x + 3*sv[0]), ld3(G.x + 3*sv[1]), ld3(G.x + 3*sv[2]), g, H);
-        } else if (type == T_EE) {
-            d2_ee_line_full(ld3(G.x + 3*sv[0]), ld3(G.x + 3*sv[1]), ld3(G.x + 3*sv[2]), ld3(G.x + 3*sv[3]), g, H);
-        } else {
-            d2_pt_plane_full(ld3(G.x + 3*sv[0]), ld3(G.x + 3*sv[1]), ld3(G.x + 3*sv[2]), ld3(G.x + 3*sv[3]), g, H);
+        if (type < 0) continue;                       // warp-uniform
+        if (lane == 0) {
+            int4 s4 = cst[c];
+            int sv[4] = {s4.x, s4.y, s4.z, s4.w};
+            C.type = type;
+            C.np = stencil_np(type);
+            for (int i = 0; i < 4; i++) C.v[i] = sv[i];
+            int nx = type == T_PG ? 1 : C.np;
+            for (int i = 0; i < nx; i++) {
+                int v = sv[i];
+                for (int k = 0; k < 3; k++) C.x[3*i+k] = G.x[3*v+k];
+                C.vb[i] = G.vbody[v];
+                C.J[i][0] = 1.0; C.J[i][1] = G.xbar[3*v]; C.J[i][2] = G.xbar[3*v+1]; C.J[i][3] = G.xbar[3*v+2];
+            }
+            barrier3(barrier, cxb[c], dhat * dhat, C.B0, C.B1, C.B2);
+            C.bodies[0] = C.vb[0]; C.nbd = 1;
+            for (int i = 1; i < C.np; i++) if (C.vb[i] != C.bodies[0]) { C.bodies[1] = C.vb[i]; C.nbd = 2; break; }
         }
-        double B0, B1, B2;
-        barrier3(barrier, cxb[c], dhat * dhat, B0, B1, B2);
+        __syncwarp();
+        warp_distance_derivs(C, G);
+        const int np = C.np, m = 3 * np;
+        const double B1 = C.B1, B2 = C.B2;
+        double* A = C.E.A;
         if (hess_mode == ABD_HESS_REFERENCE) {
-            if (type == T_EE) psd_project(12, H);                     // abd.py:247
-            for (int i = 0; i < m; i++)
-                for (int j = 0; j < m; j++) {
-                    double h = (type == T_PP) ? 0.0 : B1 * H[i*m+j];  // abd.py:381-382
-                    H[i*m+j] = (h + B2 * g[i] * g[j]) * sc;
-                }
+            if (C.type == T_EE) warp_psd_project(C.E, 12);               // abd.py:247
+            for (int e = lane; e < m * m; e += 32) {
+                int i = e / m, j = e % m;
+                double h = (C.type == T_PP) ? 0.0 : B1 * A[i*12+j];       // abd.py:381-382
+                A[i*12+j] = (h + B2 * C.g[i] * C.g[j]) * sc;
+            }
+            __syncwarp();
         } else {
-            for (int i = 0; i < m; i++)
-                for (int j = 0; j < m; j++) H[i*m+j] = B1 * H[i*m+j] + B2 * g[i] * g[j];
-            psd_project(m, H);
-            for (int i = 0; i < m * m; i++) H[i] *= sc;
+            for (int e = lane; e < m * m; e += 32) {
+                int i = e / m, j = e % m;
+                A[i*12+j] = B1 * A[i*12+j] + B2 * C.g[i] * C.g[j];
+            }
+            __syncwarp();
+            warp_psd_project(C.E, m);
+            for (int e = lane; e < m * m; e += 32) { int i = e / m, j = e % m; A[i*12+j] *= sc; }
+            __syncwarp();
         }
-        for (int i = 0; i < m; i++) g[i] *= B1 * sc;
-        // gradient: G[b] += J_v^T g_v for dynamic bodies
-        int vb[4]; double Jv[4][4];
-        for (int i = 0; i < np; i++) {
-            int v = sv[i];
-            vb[i] = G.vbody[v];
-            Jv[i][0] = 1.0; Jv[i][1] = G.xbar[3*v]; Jv[i][2] = G.xbar[3*v+1]; Jv[i][3] = G.xbar[3*v+2];
-            if (!(G.mass[vb[i]] > 0.0)) continue;
-            double* gb = grad + 12 * vb[i];
-            for (int a = 0; a < 4; a++)
-                for (int k = 0; k < 3; k++) atomicAdd(gb + 3*a + k, Jv[i][a] * g[3*i+k]);
+        // gradient: G[b][3 al + k] += J_i[al] g_i[k] * B1 * sc for dynamic bodies
+        for (int e = lane; e < np * 12; e += 32) {
+            int i = e / 12, al = (e % 12) / 3, k = e % 3;
+            int b = C.vb[i];
+            if (G.mass[b] > 0.0) atomicAdd(grad + 12L * b + 3 * al + k, C.J[i][al] * C.g[3*i+k] * B1 * sc);
         }
-        // Hessian: distinct body pairs among the stencil (at most 2 bodies)
-        int bodies[2] = {vb[0], vb[0]}; int nbd = 1;
-        for (int i = 1; i < np; i++) if (vb[i] != bodies[0]) { bodies[1] = vb[i]; nbd = 2; break; }
-        for (int pa = 0; pa < nbd; pa++)
-            for (int pb = 0; pb < nbd; pb++) {
-                int Ba = bodies[pa], Bb = bodies[pb];
+        // Hessian blocks of the (at most two) bodies
+        for (int pa = 0; pa < C.nbd; pa++)
+            for (int pb = 0; pb < C.nbd; pb++) {
+                int Ba = C.bodies[pa], Bb = C.bodies[pb];
                 if (!(G.mass[Ba] > 0.0) || !(G.mass[Bb] > 0.0)) continue;
                 int bi = find_block(row_ptr, bcol, Ba, Bb);
                 if (bi < 0) continue;
                 T* V = vals + (long)bi * 144;
-                for (int al = 0; al < 4; al++)
-                    for (int be = 0; be < 4; be++)
-                        for (int r = 0; r < 3; r++)
-                            for (int q = 0; q < 3; q++) {
-                                double sum = 0;
-                                for (int i = 0; i < np; i++) {
-                                    if (vb[i] != Ba) continue;
-                                    for (int j = 0; j < np; j++) {
-                                        if (vb[j] != Bb) continue;
-                                        sum += Jv[i][al] * Jv[j][be] * H[(3*i+r)*m + 3*j+q];
-                                    }
-                                }
-                                if (sum != 0.0) atomicAdd(V + (3*be+q)*12 + 3*al+r, (T)sum);
-                            }
+                for (int e = lane; e < 144; e += 32) {
+                    int row = e % 12, col = e / 12;          // column-major block entry (row, col)
+                    int al = row / 3, r = row % 3, be = col / 3, q = col % 3;
+                    double sum = 0;
+                    for (int i = 0; i < np; i++) {
+                        if (C.vb[i] != Ba) continue;
+                        for (int j = 0; j < np; j++) {
+                            if (C.vb[j] != Bb) continue;
+                            sum += C.J[i][al] * C.J[j][be] * A[(3*i+r)*12 + 3*j+q];
+                        }
+                    }
+                    if (sum != 0.0) atomicAdd(V + e, (T)sum);
+                }
             }
+        __syncwarp();
     }
 }
 
@@ -271,6 +433,7 @@ int eng_assemble(Engine* E) {
     // counters were synchronised by the caller after detection
     int n = E->hcnt->n_total;
     int nkeys = nb + 2 * n;
+    int ph = phase_begin(E, PH_ASM_KEYS);
     CUDA_TRY(cudaMemsetAsync(&E->dcnt->n_active, 0, sizeof(int), s));
     k_diag_keys<<<grid_for(nb), 256, 0, s>>>(nb, E->keys);
     k_contact_prepare<<<grid_for(n > 0 ? n : 1, 128), 128, 0, s>>>(E->dcnt, E->contacts, G, P.ee_f32, P.dhat, nb, E->cst,
@@ -288,27 +451,36 @@ int eng_assemble(Engine* E) {
     E->nnzb_host = nnzb;
     if (nnzb > E->blk_cap) { if ((rc = eng_grow_blocks(E, nnzb))) return rc; }
     k_block_rows<<<grid_for(nnzb), 256, 0, s>>>(nb, E->ukeys, n_unique, E->row_ptr, E->bcol, E->dcnt);
+    phase_end(E, ph, 0);
     double sc = P.kappa * P.dt * P.dt;
     if (E->mixed) {
         float* V = (float*)E->vals;
         k_zero_vals<float><<<grid_for((long)nnzb * 144), 256, 0, s>>>(E->dcnt, V);
-        k_body_assemble<float><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->st, E->mass, E->J, P.dt, P.gravity[0], P.gravity[1], P.gravity[2],
+        k_body_assemble<float><<<grid_for(32L * nb, 32 * BA_WARPS), 32 * BA_WARPS, 0, s>>>(nb, E->st, E->mass, E->J, P.dt, P.gravity[0], P.gravity[1], P.gravity[2],
                                                                P.k_ortho, P.hess_mode == ABD_HESS_PROJECTED, P.pinned_diag,
                                                                E->row_ptr, E->bcol, V, E->g);
         if (n > 0)
-            k_contact_assemble<float><<<grid_for(n, 64), 64, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
+            k_contact_assemble<float><<<grid_for(32L * n, 32 * CA_WARPS), 32 * CA_WARPS, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
                                                                      P.hess_mode, E->row_ptr, E->bcol, V, E->g);
-        k_block_inverse<float><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (float*)E->dinv);
+        if (!eng_solver_is_direct(E))
+            k_block_inverse<float><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (float*)E->dinv);
     } else {
         double* V = (double*)E->vals;
         k_zero_vals<double><<<grid_for((long)nnzb * 144), 256, 0, s>>>(E->dcnt, V);
-        k_body_assemble<double><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->st, E->mass, E->J, P.dt, P.gravity[0], P.gravity[1], P.gravity[2],
+        int p1 = phase_begin(E, PH_ASM_BODY);
+        k_body_assemble<double><<<grid_for(32L * nb, 32 * BA_WARPS), 32 * BA_WARPS, 0, s>>>(nb, E->st, E->mass, E->J, P.dt, P.gravity[0], P.gravity[1], P.gravity[2],
                                                                 P.k_ortho, P.hess_mode == ABD_HESS_PROJECTED, P.pinned_diag,
                                                                 E->row_ptr, E->bcol, V, E->g);
+        phase_end(E, p1, 0);
+        int p2 = phase_begin(E, PH_ASM_CONTACT);
         if (n > 0)
-            k_contact_assemble<double><<<grid_for(n, 64), 64, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
+            k_contact_assemble<double><<<grid_for(32L * n, 32 * CA_WARPS), 32 * CA_WARPS, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
                                                                       P.hess_mode, E->row_ptr, E->bcol, V, E->g);
-        k_block_inverse<double><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (double*)E->dinv);
+        phase_end(E, p2, 0);
+        int p3 = phase_begin(E, PH_ASM_INV);
+        if (!eng_solver_is_direct(E))
+            k_block_inverse<double><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (double*)E->dinv);
+        phase_end(E, p3, 0);
     }
     double* gg = E->scd + SD_GG * E->ns;
     CUDA_TRY(cudaMemsetAsync(gg, 0, sizeof(double) * E->ns, s));

@@ -182,7 +182,8 @@ struct Engine {
     int fail(int code, const std::string& m) { err = m; return code; }
 };
 
-enum { PH_DETECT = 0, PH_ASSEMBLE, PH_SOLVE, PH_ENERGY, PH_CCD, PH_OTHER, PH_EQUERY, PH_SPMV };
+enum { PH_DETECT = 0, PH_ASSEMBLE, PH_SOLVE, PH_ENERGY, PH_CCD, PH_OTHER, PH_EQUERY, PH_SPMV,
+       PH_ASM_KEYS, PH_ASM_BODY, PH_ASM_CONTACT, PH_ASM_INV, PH_DENSE, PH_SWEPT, PH_ELIST, PH_TRIALS };
 
 // Bracket device work with events when timing is on.  phase_begin returns a
 // record index (or -1), phase_end closes it with the algorithmic bytes moved.

@@ -325,7 +325,7 @@ DV void psd_project(int n, double* H) {
         for (int p = 0; p < n; p++)
             for (int q = p + 1; q < n; q++) {
                 double apq = A[p*n+q];
-                if (fabs(apq) <= 1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])) + 1e-300 * fro) continue;
+                if (fabs(apq) <= fmax(1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])), 1e-16 * sqrt(fro))) continue;
                 rotated = 1;
                 double theta = (A[q*n+q] - A[p*n+p]) / (2 * apq);
                 double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));

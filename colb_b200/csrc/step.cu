@@ -163,7 +163,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             st.n_active = E->hcnt->n_active;
             // candidates along x -> x - J du, shared by CCD, every energy
             // of the line search and the next detection
-            { int ph = phase_begin(E, PH_DETECT); rc = eng_swept(E, E->du, -1.0, done); phase_end(E, ph, 0); if (rc) return rc; }
+            { int ph = phase_begin(E, PH_SWEPT); rc = eng_swept(E, E->du, -1.0, done); phase_end(E, ph, 0); if (rc) return rc; }
             if (P.ccd) {
                 int ph = phase_begin(E, PH_CCD); rc = eng_ccd_list(E, done); phase_end(E, ph, 0);
                 if (rc) return rc;
@@ -174,6 +174,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             E->launches++;
             k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
             E->launches++;
+            int ph_tr = phase_begin(E, PH_TRIALS);
             for (int trial = 0; trial < 64; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
                 { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
@@ -183,6 +184,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
                 if ((rc = eng_sync_counters(E))) return rc;
                 if (E->hcnt->ls_pending == 0) break;
             }
+            phase_end(E, ph_tr, 0);
             k_newton_book<<<1, 256, 0, s>>>(ns, done, iter, E->scd + SD_GG * ns, alpha, prof_res, prof_alpha, mi,
                                             P.newton_tol, E->dcnt);
             E->launches++;

@@ -337,7 +337,7 @@ int eng_energy_list(Engine* E, int slot, const int* skip) {
     if (rc) return rc;
     if ((rc = eng_body_energy(E, Eo, skip))) return rc;
     if (E->n_sw > 0) {
-        int ph = phase_begin(E, PH_EQUERY);
+        int ph = phase_begin(E, PH_ELIST);
         k_list_energy<<<grid_for(E->n_sw, 128), 128, 0, s>>>(E->n_sw, E->sw, eng_geo(E), E->bscene, skip, P.ee_f32, P.dhat,
                                                              P.barrier, P.kappa * P.dt * P.dt, Eo);
         // per listed pair: the entry, its 2-4 vertex ids and positions

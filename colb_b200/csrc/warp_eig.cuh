@@ -1,0 +1,124 @@
+// warp_eig.cuh — one warp projects a small symmetric matrix (n <= 12) held
+// in shared memory onto the PSD cone: V max(L, 0) V^T.
+//
+// Parallel cyclic Jacobi with round-robin ("tournament") pair ordering:
+// each round rotates n/2 disjoint index pairs at once, so for a product R of
+// disjoint Givens rotations every entry of R^T A R depends on at most four
+// entries of A and every lane updates its share of the entries
+// independently.  n - 1 rounds (n even; odd n gets a dummy index) make one
+// sweep.  A rotation is skipped when |a_pq| is at rounding level against its
+// diagonal pair or against the whole matrix (rank-deficient Hessians drive
+// some diagonals to zero); sweeps stop when none was applied, the same
+// criterion the serial oracle uses.
+#pragma once
+#include "common.cuh"
+
+struct WarpEigSmem {
+    double A[144];       // matrix, row-major n x n (ld 12)
+    double T[144];       // scratch
+    double V[144];       // eigenvectors
+    double c[6], s[6];   // rotation of each pair this round
+    int partner[12];     // partner of each index this round (-1 none)
+    int role[12];        // 0: index is p of its pair, 1: index is q
+    int pair_of[12];
+    int flag;
+};
+
+// pairs of round r in a tournament of m players (m even): player m-1 fixed,
+// the others rotate
+DV void tournament_pair(int m, int r, int k, int& p, int& q) {
+    if (k == 0) { p = m - 1; q = r % (m - 1); }
+    else {
+        p = (r + k) % (m - 1);
+        q = (r - k + (m - 1)) % (m - 1);
+    }
+    if (p > q) { int t = p; p = q; q = t; }
+}
+
+// Project S.A (n x n, ld 12) in place.  All 32 lanes call it.
+DV void warp_psd_project(WarpEigSmem& S, int n) {
+    const int lane = threadIdx.x & 31;
+    const int m = (n & 1) ? n + 1 : n;      // players, index n is a dummy when n is odd
+    for (int e = lane; e < 144; e += 32) { int i = e / 12, j = e % 12; S.V[e] = (i == j) ? 1.0 : 0.0; }
+    // scale for the all-zero test
+    double fro = 0;
+    for (int e = lane; e < n * n; e += 32) { int i = e / n, j = e % n; fro += S.A[i*12+j] * S.A[i*12+j]; }
+    for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+    if (fro == 0.0) return;
+    __syncwarp();
+    for (int sweep = 0; sweep < 50; sweep++) {
+        if (lane == 0) S.flag = 0;
+        __syncwarp();
+        for (int r = 0; r < m - 1; r++) {
+            // rotation angles of this round's pairs
+            if (lane < m / 2) {
+                int p, q; tournament_pair(m, r, lane, p, q);
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    double apq = S.A[p*12+q], app = S.A[p*12+p], aqq = S.A[q*12+q];
+                    if (fabs(apq) > fmax(1e-15 * sqrt(fabs(app * aqq)), 1e-16 * sqrt(fro))) {
+                        double theta = (aqq - app) / (2 * apq);
+                        double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+                        c = rsqrt(t * t + 1); s = t * c;
+                        S.flag = 1;
+                    }
+                    S.partner[p] = q; S.partner[q] = p; S.role[p] = 0; S.role[q] = 1;
+                    S.pair_of[p] = lane; S.pair_of[q] = lane;
+                } else if (p < n) {
+                    S.partner[p] = -1;
+                }
+                S.c[lane] = c; S.s[lane] = s;
+            }
+            __syncwarp();
+            // column j of R: R[j][j] = c, R[partner][j] = -s if j is p, +s if j is q.
+            // pass 1: T = R^T A R; every entry reads at most four entries of A
+            for (int e = lane; e < n * n; e += 32) {
+                int i = e / n, j = e % n;
+                int pi = S.partner[i], pj = S.partner[j];
+                double ci = 1, si = 0, cj = 1, sj = 0;
+                if (pi >= 0) { ci = S.c[S.pair_of[i]]; si = S.role[i] == 0 ? -S.s[S.pair_of[i]] : S.s[S.pair_of[i]]; }
+                if (pj >= 0) { cj = S.c[S.pair_of[j]]; sj = S.role[j] == 0 ? -S.s[S.pair_of[j]] : S.s[S.pair_of[j]]; }
+                double v = ci * cj * S.A[i*12+j];
+                if (pj >= 0) v += ci * sj * S.A[i*12+pj];
+                if (pi >= 0) v += si * cj * S.A[pi*12+j];
+                if (pi >= 0 && pj >= 0) v += si * sj * S.A[pi*12+pj];
+                S.T[i*12+j] = v;
+            }
+            __syncwarp();
+            // pass 2: V R into A (free now that T holds the rotated matrix)
+            for (int e = lane; e < n * n; e += 32) {
+                int i = e / n, j = e % n;
+                int pj = S.partner[j];
+                double cj = 1, sj = 0;
+                if (pj >= 0) { cj = S.c[S.pair_of[j]]; sj = S.role[j] == 0 ? -S.s[S.pair_of[j]] : S.s[S.pair_of[j]]; }
+                double w = cj * S.V[i*12+j];
+                if (pj >= 0) w += sj * S.V[i*12+pj];
+                S.A[i*12+j] = w;
+            }
+            __syncwarp();
+            // pass 3: swap back
+            for (int e = lane; e < n * n; e += 32) {
+                int i = e / n, j = e % n;
+                double a = S.T[i*12+j], v = S.A[i*12+j];
+                S.V[i*12+j] = v;
+                S.A[i*12+j] = a;
+            }
+            __syncwarp();
+            if (lane < 12) { S.partner[lane] = -1; }
+            __syncwarp();
+        }
+        if (!S.flag) break;
+        __syncwarp();
+    }
+    __syncwarp();
+    // H = V max(L,0) V^T into T, then back into A
+    for (int e = lane; e < n * n; e += 32) {
+        int i = e / n, j = e % n;
+        double acc = 0;
+        for (int k = 0; k < n; k++) { double l = S.A[k*12+k]; if (l > 0) acc += S.V[i*12+k] * l * S.V[j*12+k]; }
+        S.T[i*12+j] = acc;
+    }
+    __syncwarp();
+    for (int e = lane; e < n * n; e += 32) { int i = e / n, j = e % n; S.A[i*12+j] = S.T[i*12+j]; }
+    __syncwarp();
+}

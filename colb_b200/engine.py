@@ -23,7 +23,8 @@ EXPORTS = [
     "abd_count_intersections", "abd_last_error", "abd_abi_version", "abd_set_timing", "abd_get_timing",
     "abd_ee_pairs_static",
 ]
-PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv"]
+PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv", "asm_keys", "asm_body",
+          "asm_contact", "asm_inverse", "dense", "swept", "energy_list", "ls_trials"]
 
 
 class AbdError(RuntimeError):

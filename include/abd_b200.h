@@ -223,14 +223,15 @@ int abd_count_intersections(AbdHandle* h, int32_t* count);
 /* Device-side phase timers (no reference counterpart; the reference wraps
  * step() in wp.ScopedTimer, abd.py:676).  When on, every phase launch is
  * bracketed by CUDA events on the handle's stream and summed per phase:
- *   0 detect (transform, grid, pair list)   1 assemble (blocks, gradient)
- *   2 solve (Krylov)                        3 line-search energy
- *   4 CCD                                   5 other (bookkeeping, forward)
- *   6 contact-energy query kernels only     7 SpMV kernels only
- * abd_get_timing writes ms[8], launches[8] and the algorithmic bytes[8]
- * those phases moved (see the library's documentation of each kernel);
- * reset clears them. */
-#define ABD_NUM_PHASES 8
+ *   0 detect (pair list)        1 assemble (all of it)    2 solve
+ *   3 line-search energy        4 CCD                     5 other
+ *   6 contact-energy kernels    7 SpMV kernels            8 assembly: keys, sort, blocks
+ *   9 assembly: bodies          10 assembly: contacts     11 assembly: block inverse
+ *   12 dense factor + solve     13 swept candidate list   14 contact-energy list kernel
+ *   15 line-search trials (apply + energy + decision)
+ * abd_get_timing writes ms[16], launches[16] and the algorithmic bytes[16]
+ * those phases moved (documented at each kernel); reset clears them. */
+#define ABD_NUM_PHASES 16
 int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset);
 int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes);
 

@@ -335,13 +335,14 @@ void oracle_psd_project(int n, double* H) {
     for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) V[i*n+j] = (i == j);
     double fro = 0; for (int i = 0; i < n*n; i++) fro += A[i]*A[i];
     if (fro == 0) return;
-    /* a rotation is skipped when |a_pq| is at rounding level against the
-     * diagonal; the sweeps stop when none was applied (scale-invariant) */
+    /* a rotation is skipped when |a_pq| is at rounding level against its
+     * diagonal pair or against the whole matrix; the sweeps stop when none
+     * was applied (scale-invariant) */
     for (int sweep = 0; sweep < 50; sweep++) {
         int rotated = 0;
         for (int p = 0; p < n; p++) for (int q = p + 1; q < n; q++) {
             double apq = A[p*n+q];
-            if (fabs(apq) <= 1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])) + 1e-300 * fro) continue;
+            if (fabs(apq) <= fmax(1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])), 1e-16 * sqrt(fro))) continue;
             rotated = 1;
             double theta = (A[q*n+q] - A[p*n+p]) / (2 * apq);
             double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta*theta + 1));
