@@ -476,7 +476,9 @@ int eng_assemble(Engine* E) {
         if (n > 0)
             k_contact_assemble<double><<<grid_for(32L * n, 32 * CA_WARPS), 32 * CA_WARPS, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
                                                                       P.hess_mode, E->row_ptr, E->bcol, V, E->g);
-        phase_end(E, p2, 0);
+        // per candidate: type; per active contact: stencil, barrier argument,
+        // 4 positions + 4 rest positions, 4 body blocks and the gradient rows
+        phase_end(E, p2, 4.0 * n + E->hcnt->n_active * (16.0 + 8.0 + 96.0 + 96.0 + 4 * 1152.0 + 384.0));
         int p3 = phase_begin(E, PH_ASM_INV);
         if (!eng_solver_is_direct(E))
             k_block_inverse<double><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (double*)E->dinv);

@@ -163,7 +163,13 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             st.n_active = E->hcnt->n_active;
             // candidates along x -> x - J du, shared by CCD, every energy
             // of the line search and the next detection
-            { int ph = phase_begin(E, PH_SWEPT); rc = eng_swept(E, E->du, -1.0, done); phase_end(E, ph, 0); if (rc) return rc; }
+            {
+                int ph = phase_begin(E, PH_SWEPT);
+                rc = eng_swept(E, E->du, -1.0, done);
+                // positions, rest positions, increments per vertex; topology; the listed pairs
+                phase_end(E, ph, E->nv * (24.0 + 24.0 + 4.0) + E->nb * 96.0 + E->ne * 8.0 + E->nt * 12.0 + E->n_sw * 24.0);
+                if (rc) return rc;
+            }
             if (P.ccd) {
                 int ph = phase_begin(E, PH_CCD); rc = eng_ccd_list(E, done); phase_end(E, ph, 0);
                 if (rc) return rc;
