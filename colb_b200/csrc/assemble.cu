@@ -19,7 +19,6 @@
 #include <cub/cub.cuh>
 
 Geo eng_geo(Engine* E);
-bool eng_solver_is_direct(const Engine* E);
 
 DV int stencil_np(int type) { return type == T_PP ? 2 : (type == T_PE ? 3 : (type == T_PG ? 1 : 4)); }
 DV int other_vertex(int type, int4 s) { return type == T_EE ? s.z : (type == T_PG ? s.x : s.y); }
@@ -375,32 +374,59 @@ __global__ void __launch_bounds__(32 * CA_WARPS) k_contact_assemble(const Counte
 }
 
 // ---------------------------------------------------- block-Jacobi inverse
+// One warp per body: Gauss-Jordan with partial pivoting on [D | I] in shared
+// memory, lanes owning the 24 columns.  A singular block gives the identity.
+#define BI_WARPS 4
 template <class T>
-__global__ void k_block_inverse(int nb, const int* __restrict__ row_ptr, const int* __restrict__ bcol,
-                                const T* __restrict__ vals, T* dinv) {
-    GS_LOOP(b, nb) {
-        int bi = find_block(row_ptr, bcol, (int)b, (int)b);
+__global__ void __launch_bounds__(32 * BI_WARPS) k_block_inverse(int nb, const int* __restrict__ row_ptr,
+        const int* __restrict__ bcol, const T* __restrict__ vals, T* dinv) {
+    __shared__ double sM[BI_WARPS][12][25];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double (*M)[25] = sM[w];
+    for (int b = blockIdx.x * BI_WARPS + w; b < nb; b += gridDim.x * BI_WARPS) {
+        int bi = find_block(row_ptr, bcol, b, b);
         if (bi < 0) continue;
         const T* V = vals + (long)bi * 144;
-        double M[12][24];
-        for (int r = 0; r < 12; r++)
-            for (int c = 0; c < 24; c++) M[r][c] = c < 12 ? (double)V[c*12 + r] : (c - 12 == r ? 1.0 : 0.0);
+        for (int e = lane; e < 288; e += 32) {
+            int r = e / 24, c = e % 24;
+            M[r][c] = c < 12 ? (double)V[c*12 + r] : (c - 12 == r ? 1.0 : 0.0);
+        }
+        __syncwarp();
         bool ok = true;
-        for (int c = 0; c < 12 && ok; c++) {
-            int p = c;
-            for (int r = c + 1; r < 12; r++) if (fabs(M[r][c]) > fabs(M[p][c])) p = r;
-            if (M[p][c] == 0.0) { ok = false; break; }
-            if (p != c) for (int j = 0; j < 24; j++) { double t = M[p][j]; M[p][j] = M[c][j]; M[c][j] = t; }
-            double iv = 1.0 / M[c][c];
-            for (int j = 0; j < 24; j++) M[c][j] *= iv;
-            for (int r = 0; r < 12; r++) if (r != c) {
-                double f = M[r][c];
-                if (f != 0.0) for (int j = 0; j < 24; j++) M[r][j] -= f * M[c][j];
+        for (int c = 0; c < 12; c++) {
+            // first row of largest magnitude in column c at or below the diagonal
+            double best = lane >= c && lane < 12 ? fabs(M[lane][c]) : -1.0;
+            int p = lane;
+            for (int o = 16; o > 0; o >>= 1) {
+                double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                int op = __shfl_xor_sync(0xffffffffu, p, o);
+                if (ob > best || (ob == best && op < p)) { best = ob; p = op; }
             }
+            if (M[p][c] == 0.0) { ok = false; break; }
+            if (p != c && lane < 24) { double t = M[p][lane]; M[p][lane] = M[c][lane]; M[c][lane] = t; }
+            __syncwarp();
+            double iv = 1.0 / M[c][c];
+            __syncwarp();
+            if (lane < 24) M[c][lane] *= iv;
+            __syncwarp();
+            double f[12];
+#pragma unroll
+            for (int r = 0; r < 12; r++) f[r] = M[r][c];
+            __syncwarp();
+            if (lane < 24) {
+                double mc = M[c][lane];
+#pragma unroll
+                for (int r = 0; r < 12; r++)
+                    if (r != c && f[r] != 0.0) M[r][lane] -= f[r] * mc;
+            }
+            __syncwarp();
         }
         T* D = dinv + (long)b * 144;
-        for (int c = 0; c < 12; c++)
-            for (int r = 0; r < 12; r++) D[c*12 + r] = (T)(ok ? M[r][12 + c] : (r == c ? 1.0 : 0.0));
+        for (int e = lane; e < 144; e += 32) {
+            int c = e / 12, r = e % 12;
+            D[e] = (T)(ok ? M[r][12 + c] : (r == c ? 1.0 : 0.0));
+        }
+        __syncwarp();
     }
 }
 
@@ -462,8 +488,7 @@ int eng_assemble(Engine* E) {
         if (n > 0)
             k_contact_assemble<float><<<grid_for(32L * n, 32 * CA_WARPS), 32 * CA_WARPS, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
                                                                      P.hess_mode, E->row_ptr, E->bcol, V, E->g);
-        if (!eng_solver_is_direct(E))
-            k_block_inverse<float><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (float*)E->dinv);
+        k_block_inverse<float><<<grid_for(32L * nb, 32 * BI_WARPS), 32 * BI_WARPS, 0, s>>>(nb, E->row_ptr, E->bcol, V, (float*)E->dinv);
     } else {
         double* V = (double*)E->vals;
         k_zero_vals<double><<<grid_for((long)nnzb * 144), 256, 0, s>>>(E->dcnt, V);
@@ -480,8 +505,7 @@ int eng_assemble(Engine* E) {
         // 4 positions + 4 rest positions, 4 body blocks and the gradient rows
         phase_end(E, p2, 4.0 * n + E->hcnt->n_active * (16.0 + 8.0 + 96.0 + 96.0 + 4 * 1152.0 + 384.0));
         int p3 = phase_begin(E, PH_ASM_INV);
-        if (!eng_solver_is_direct(E))
-            k_block_inverse<double><<<grid_for(nb, 64), 64, 0, s>>>(nb, E->row_ptr, E->bcol, V, (double*)E->dinv);
+        k_block_inverse<double><<<grid_for(32L * nb, 32 * BI_WARPS), 32 * BI_WARPS, 0, s>>>(nb, E->row_ptr, E->bcol, V, (double*)E->dinv);
         phase_end(E, p3, 0);
     }
     double* gg = E->scd + SD_GG * E->ns;

@@ -253,6 +253,7 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     }
     E->nb = nb; E->nv = nv; E->ne = (int)escene.size(); E->nt = (int)tscene.size(); E->npl = npl;
     E->h_body_begin = sc_body_begin;
+    E->h_bscene = bscene;
     E->h_edges = edges; E->h_tris = tris;
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) { delete E; g_err = "stream"; return ABD_ERR_CUDA; }
     if (P.broadphase < 0 || P.broadphase > 2) { delete E; g_err = "abd_create: broadphase must be 0, 1 or 2"; return ABD_ERR_INVALID_ARG; }

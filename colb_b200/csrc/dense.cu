@@ -1,71 +1,295 @@
-// dense.cu — direct solve of the Newton system, one dense factorization per
-// scene (the reference's solver_config != "cg" branch, abd.py:637-654, which
-// factors the assembled matrix with a cuSOLVER wrapper).
+// dense.cu — direct solve of the Newton system (the reference's
+// solver_config != "cg" branch, abd.py:637-654, which factors the assembled
+// matrix with a cuSOLVER wrapper).
 //
-// The 12x12 body blocks of each scene are scattered into a dense
-// column-major matrix (16 lanes per body row, the Krylov kernels' mapping),
-// then factored with cuSOLVER: Cholesky when the Hessian is PSD-projected,
-// LU with partial pivoting for the reference's indefinite Hessian (or when
-// Cholesky reports a non-positive pivot).  Mixed precision factors in FP32.
+// The system decouples into the connected components of the body graph whose
+// edges are the off-diagonal 12x12 blocks (two dynamic bodies joined by an
+// active contact).  A component is factored on its own:
+//   - one body: the 12x12 block inverse written by the assembly;
+//   - up to SMALL_MAX_BODIES bodies: one CTA per component factors it in
+//     shared memory (blocked Cholesky by 12-wide body columns; LU with
+//     partial pivoting when a pivot is not positive), all such components
+//     in one launch;
+//   - larger components: the 12x12 blocks are scattered into a dense
+//     column-major matrix and factored with cuSOLVER (Cholesky, or LU when
+//     Cholesky reports a non-positive pivot).
+// Mixed precision factors in FP32.
 #include "engine.cuh"
 #include <cusolverDn.h>
 #include <algorithm>
 
+// Scatter the blocks of every body that belongs to a large component into
+// that component's dense column-major matrix (16 lanes per body row).
 template <class T>
 __global__ void k_blocks_to_dense(int nb, const int* __restrict__ row_ptr, const int* __restrict__ bcol,
-                                  const T* __restrict__ vals, const int* __restrict__ bscene,
-                                  const int* __restrict__ sc_body_begin, const long long* __restrict__ dense_off,
-                                  const int* __restrict__ ndone, T* dense) {
+                                  const T* __restrict__ vals, const int* __restrict__ bcomp,
+                                  const int* __restrict__ blocal, const long long* __restrict__ comp_off,
+                                  const long long* __restrict__ comp_n, int only_c, T* dense) {
     for (long base = (long)blockIdx.x * blockDim.x; base < (long)nb * 16; base += (long)gridDim.x * blockDim.x) {
         long t = base + threadIdx.x;
         int b = (int)(t / 16), l = (int)(t % 16);
         if (b >= nb || l >= 12) continue;
-        int s = bscene[b];
-        if (ndone[s]) continue;
-        int b0 = sc_body_begin[s];
-        long n = 12L * (sc_body_begin[s + 1] - b0);
-        T* A = dense + dense_off[s];
-        long row = 12L * (b - b0) + l;
+        int c = bcomp[b];
+        if (c < 0 || (only_c >= 0 && c != only_c)) continue;
+        long n = comp_n[c];
+        T* A = dense + comp_off[c];
+        long row = 12L * blocal[b] + l;
         for (int k = row_ptr[b]; k < row_ptr[b + 1]; k++) {
-            long colb = 12L * (bcol[k] - b0);
+            long colb = 12L * blocal[bcol[k]];
             const T* V = vals + (long)k * 144 + l;
 #pragma unroll
             for (int j = 0; j < 12; j++) A[(colb + j) * n + row] = V[j * 12];
         }
     }
 }
+// right-hand sides of large components, gathered in component order
 template <class T>
-__global__ void k_rhs_cast(int n, const double* __restrict__ g, T* x) { GS_LOOP(i, n) x[i] = (T)g[i]; }
+__global__ void k_rhs_gather(int nb, const double* __restrict__ g, const int* __restrict__ bcomp,
+                             const int* __restrict__ blocal, const long long* __restrict__ comp_rhs, T* x) {
+    GS_LOOP(i, 12L * nb) {
+        int b = (int)(i / 12), c = bcomp[b];
+        if (c >= 0) x[comp_rhs[c] + 12L * blocal[b] + i % 12] = (T)g[i];
+    }
+}
+// du of every body: large components from their dense solution, single
+// bodies from their 12x12 block inverse (column-major); bodies of small
+// components (bcomp -2) were written by k_small_solve
 template <class T>
-__global__ void k_rhs_back(int n, const T* __restrict__ x, const int* __restrict__ bscene, const int* __restrict__ ndone,
-                           double* du) {
-    GS_LOOP(i, n) { if (!ndone[bscene[i / 12]]) du[i] = (double)x[i]; }
+__global__ void k_du_scatter(int nb, const double* __restrict__ g, const int* __restrict__ bcomp,
+                             const int* __restrict__ blocal, const long long* __restrict__ comp_rhs,
+                             const T* __restrict__ x, const T* __restrict__ dinv, const int* __restrict__ bscene,
+                             const int* __restrict__ ndone, double* du) {
+    GS_LOOP(i, 12L * nb) {
+        int b = (int)(i / 12), r = (int)(i % 12);
+        if (ndone[bscene[b]]) continue;
+        int c = bcomp[b];
+        if (c == -2) continue;
+        if (c >= 0) { du[i] = (double)x[comp_rhs[c] + 12L * blocal[b] + r]; continue; }
+        const T* D = dinv + 144L * b;
+        double acc = 0;
+#pragma unroll
+        for (int k = 0; k < 12; k++) acc += (double)D[k * 12 + r] * g[12L * b + k];
+        du[i] = acc;
+    }
+}
+
+constexpr int SMALL_MAX_BODIES = 12;
+constexpr int SMALL_THREADS = 256;
+
+// Load the blocks of the component's bodies (local order sb[0..nbod)) into
+// the row-major n x n matrix A (leading dimension ld) and g into x.
+template <class T>
+__device__ void small_fill(int nbod, int n, int ld, const int* sb, const int* __restrict__ blocal,
+                           const int* __restrict__ row_ptr, const int* __restrict__ bcol, const T* __restrict__ vals,
+                           const double* __restrict__ g, T* A, T* x) {
+    for (int e = threadIdx.x; e < n * ld; e += blockDim.x) A[e] = 0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = warp; i < nbod; i += nw) {
+        int b = sb[i];
+        for (int k = row_ptr[b]; k < row_ptr[b + 1]; k++) {
+            int j = blocal[bcol[k]];
+            const T* V = vals + (long)k * 144;
+            for (int e = lane; e < 144; e += 32) {
+                int cc = e / 12, r = e % 12;        // blocks are column-major
+                A[(12 * i + r) * ld + 12 * j + cc] = V[e];
+            }
+        }
+        if (lane < 12) x[12 * i + lane] = (T)g[12L * b + lane];
+    }
+    __syncthreads();
+}
+
+// One CTA per small component: A du = g in shared memory.  status bit 0 is
+// set when a component is singular (its du is zero).
+template <class T>
+__global__ void __launch_bounds__(SMALL_THREADS) k_small_solve(int nsmall, const int* __restrict__ sptr,
+        const int* __restrict__ sbody, const int* __restrict__ blocal, const int* __restrict__ row_ptr,
+        const int* __restrict__ bcol, const T* __restrict__ vals, const double* __restrict__ g, int try_chol,
+        double* du, int* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int flag, piv;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = blockIdx.x; c < nsmall; c += gridDim.x) {
+        const int* sb = sbody + sptr[c];
+        const int nbod = sptr[c + 1] - sptr[c], n = 12 * nbod, ld = n + 1;
+        T* A = (T*)smem_raw;
+        T* x = A + n * ld;
+        small_fill<T>(nbod, n, ld, sb, blocal, row_ptr, bcol, vals, g, A, x);
+        if (tid == 0) flag = try_chol ? 0 : 1;
+        __syncthreads();
+        // blocked right-looking Cholesky, lower triangle, 12-wide body columns;
+        // flag is written by warp 0 in the diagonal step only and read right
+        // after the barrier that follows it, so every thread takes the same branch
+        for (int K = 0; try_chol && K < nbod; K++) {
+            const int kb = 12 * K;
+            if (warp == 0) {
+                for (int j = 0; j < 12; j++) {
+                    if (lane == 0) {
+                        T d = A[(kb + j) * ld + kb + j];
+                        if (!(d > (T)0)) flag = 1;
+                        A[(kb + j) * ld + kb + j] = d > (T)0 ? sqrt(d) : (T)1;
+                    }
+                    __syncwarp();
+                    T djj = A[(kb + j) * ld + kb + j];
+                    if (lane > j && lane < 12) A[(kb + lane) * ld + kb + j] /= djj;
+                    __syncwarp();
+                    if (lane > j && lane < 12) {
+                        T lij = A[(kb + lane) * ld + kb + j];
+                        for (int cc = j + 1; cc <= lane; cc++) A[(kb + lane) * ld + kb + cc] -= lij * A[(kb + cc) * ld + kb + j];
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            if (flag) break;
+            // panel: rows below solve L_ik D^T = A_ik
+            for (int i = kb + 12 + tid; i < n; i += blockDim.x) {
+                T* Ri = A + i * ld + kb;
+                for (int j = 0; j < 12; j++) {
+                    T a = Ri[j];
+                    for (int t = 0; t < j; t++) a -= Ri[t] * A[(kb + j) * ld + kb + t];
+                    Ri[j] = a / A[(kb + j) * ld + kb + j];
+                }
+            }
+            __syncthreads();
+            // trailing update of the lower triangle
+            const int m = n - kb - 12;
+            for (int e = tid; e < m * m; e += blockDim.x) {
+                int i = kb + 12 + e / m, j = kb + 12 + e % m;
+                if (j > i) continue;
+                const T* Li = A + i * ld + kb;
+                const T* Lj = A + j * ld + kb;
+                T acc = 0;
+#pragma unroll
+                for (int t = 0; t < 12; t++) acc += Li[t] * Lj[t];
+                A[i * ld + j] -= acc;
+            }
+            __syncthreads();
+        }
+        if (!flag) {
+            // L y = g, then L^T du = y
+            for (int K = 0; K < nbod; K++) {
+                const int kb = 12 * K;
+                if (tid == 0)
+                    for (int j = 0; j < 12; j++) {
+                        T a = x[kb + j];
+                        for (int t = 0; t < j; t++) a -= A[(kb + j) * ld + kb + t] * x[kb + t];
+                        x[kb + j] = a / A[(kb + j) * ld + kb + j];
+                    }
+                __syncthreads();
+                for (int i = kb + 12 + tid; i < n; i += blockDim.x) {
+                    T acc = 0;
+                    for (int t = 0; t < 12; t++) acc += A[i * ld + kb + t] * x[kb + t];
+                    x[i] -= acc;
+                }
+                __syncthreads();
+            }
+            for (int K = nbod - 1; K >= 0; K--) {
+                const int kb = 12 * K;
+                if (tid == 0)
+                    for (int j = 11; j >= 0; j--) {
+                        T a = x[kb + j];
+                        for (int t = j + 1; t < 12; t++) a -= A[(kb + t) * ld + kb + j] * x[kb + t];
+                        x[kb + j] = a / A[(kb + j) * ld + kb + j];
+                    }
+                __syncthreads();
+                for (int i = tid; i < kb; i += blockDim.x) {
+                    T acc = 0;
+                    for (int t = 0; t < 12; t++) acc += A[(kb + t) * ld + i] * x[kb + t];
+                    x[i] -= acc;
+                }
+                __syncthreads();
+            }
+        } else {
+            // LU with partial pivoting on a fresh copy
+            small_fill<T>(nbod, n, ld, sb, blocal, row_ptr, bcol, vals, g, A, x);
+            bool singular = false;
+            for (int k = 0; k < n; k++) {
+                if (warp == 0) {
+                    T best = -1; int bi = k;
+                    for (int i = k + lane; i < n; i += 32) {
+                        T v = fabs(A[i * ld + k]);
+                        if (v > best) { best = v; bi = i; }
+                    }
+                    for (int o = 16; o > 0; o >>= 1) {
+                        T ob = __shfl_xor_sync(0xffffffffu, best, o);
+                        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+                    }
+                    if (lane == 0) piv = bi;
+                }
+                __syncthreads();
+                const int p = piv;
+                if (p != k) {
+                    for (int j = tid; j < n; j += blockDim.x) { T t = A[k * ld + j]; A[k * ld + j] = A[p * ld + j]; A[p * ld + j] = t; }
+                    if (tid == 0) { T t = x[k]; x[k] = x[p]; x[p] = t; }
+                }
+                __syncthreads();
+                const T pv = A[k * ld + k];
+                if (pv == (T)0) { singular = true; break; }
+                for (int i = k + 1 + tid; i < n; i += blockDim.x) A[i * ld + k] /= pv;
+                __syncthreads();
+                const int m = n - k - 1;
+                for (int e = tid; e < m * m; e += blockDim.x) {
+                    int i = k + 1 + e / m, j = k + 1 + e % m;
+                    A[i * ld + j] -= A[i * ld + k] * A[k * ld + j];
+                }
+                __syncthreads();
+            }
+            if (singular) {
+                for (int i = tid; i < n; i += blockDim.x) x[i] = 0;
+                if (tid == 0) atomicOr(status, 1);
+                __syncthreads();
+            } else {
+                for (int k = 0; k < n; k++) {
+                    const T xk = x[k];
+                    for (int i = k + 1 + tid; i < n; i += blockDim.x) x[i] -= A[i * ld + k] * xk;
+                    __syncthreads();
+                }
+                for (int k = n - 1; k >= 0; k--) {
+                    if (tid == 0) x[k] /= A[k * ld + k];
+                    __syncthreads();
+                    const T xk = x[k];
+                    for (int i = tid; i < k; i += blockDim.x) x[i] -= A[i * ld + k] * xk;
+                    __syncthreads();
+                }
+            }
+        }
+        for (int i = tid; i < n; i += blockDim.x) du[12L * sb[i / 12] + i % 12] = (double)x[i];
+        __syncthreads();
+    }
 }
 
 struct DenseState {
     cusolverDnHandle_t h = nullptr;
     void* A = nullptr; size_t A_bytes = 0;
-    void* work = nullptr; size_t work_bytes = 0;
-    int* ipiv = nullptr; int ipiv_n = 0;
-    int* info = nullptr;
-    long long* off_d = nullptr;
-    std::vector<long long> off;
-    std::vector<int> n;
-    void* rhs = nullptr;
+    void* rhs = nullptr; size_t rhs_bytes = 0;
+    void* work = nullptr; size_t work_bytes = 0; int work_n = 0;
+    int* ipiv = nullptr;
+    int* info = nullptr;                             // [0] small-component status, then 2 per large component
+    long long* comp_d = nullptr;                     // per large component: offset | rhs offset | n
+    int* imap_d = nullptr; int* imap_h = nullptr;    // bmap | blocal | sptr | sbody, pinned staging
+    std::vector<unsigned long long> keys;
+    std::vector<int> done, parent, size, root, bmap, fill;
+    bool smem_set[2] = {false, false};
 };
 static DenseState* ds_of(Engine* E) { return reinterpret_cast<DenseState*>(E->dense_state); }
+
+constexpr int MAX_LARGE_COMPONENTS = 16;
 
 void eng_dense_free(Engine* E) {
     DenseState* D = ds_of(E);
     if (!D) return;
     if (D->h) cusolverDnDestroy(D->h);
-    void* ps[] = {D->A, D->work, D->ipiv, D->info, D->off_d, D->rhs};
+    void* ps[] = {D->A, D->rhs, D->work, D->ipiv, D->info, D->comp_d, D->imap_d};
     for (void* p : ps) if (p) cudaFree(p);
+    if (D->imap_h) cudaFreeHost(D->imap_h);
     delete D;
     E->dense_state = nullptr;
 }
 
-// bytes the dense path needs (matrices only)
+// bytes of the dense matrices if every scene were one component
 long long eng_dense_bytes(Engine* E) {
     long long tot = 0;
     for (int s = 0; s < E->ns; s++) {
@@ -81,127 +305,220 @@ static int dense_init(Engine* E) {
     E->dense_state = D;
     if (cusolverDnCreate(&D->h) != CUSOLVER_STATUS_SUCCESS) return E->fail(ABD_ERR_CUDA, "cusolverDnCreate");
     cusolverDnSetStream(D->h, E->stream);
-    long long tot = 0;
-    int nmax = 0;
-    for (int s = 0; s < E->ns; s++) {
-        int n = 12 * (E->h_body_begin[s + 1] - E->h_body_begin[s]);
-        D->off.push_back(tot); D->n.push_back(n);
-        tot += (long long)n * n;
-        nmax = std::max(nmax, n);
-    }
-    size_t es = E->mixed ? 4 : 8;
-    D->A_bytes = (size_t)tot * es;
-    if (cudaMalloc(&D->A, D->A_bytes) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc dense matrices");
-    if (cudaMalloc(&D->off_d, sizeof(long long) * E->ns) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc");
-    cudaMemcpy(D->off_d, D->off.data(), sizeof(long long) * E->ns, cudaMemcpyHostToDevice);
-    if (cudaMalloc(&D->ipiv, sizeof(int) * nmax) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc ipiv");
-    D->ipiv_n = nmax;
-    if (cudaMalloc(&D->info, sizeof(int) * 2) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc info");
-    if (cudaMalloc(&D->rhs, es * 12 * (size_t)E->nb) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc rhs");
-    // workspace for the largest scene, both factorizations
-    int lw1 = 0, lw2 = 0;
-    if (E->mixed) {
-        cusolverDnSpotrf_bufferSize(D->h, CUBLAS_FILL_MODE_LOWER, nmax, (float*)D->A, std::max(nmax, 1), &lw1);
-        cusolverDnSgetrf_bufferSize(D->h, nmax, nmax, (float*)D->A, std::max(nmax, 1), &lw2);
-    } else {
-        cusolverDnDpotrf_bufferSize(D->h, CUBLAS_FILL_MODE_LOWER, nmax, (double*)D->A, std::max(nmax, 1), &lw1);
-        cusolverDnDgetrf_bufferSize(D->h, nmax, nmax, (double*)D->A, std::max(nmax, 1), &lw2);
-    }
-    D->work_bytes = (size_t)std::max(lw1, lw2) * es + 256;
-    if (cudaMalloc(&D->work, D->work_bytes) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc cusolver work");
+    size_t ni = 4 * (size_t)E->nb + 8;
+    if (cudaMalloc(&D->imap_d, sizeof(int) * ni) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc maps");
+    if (cudaMallocHost(&D->imap_h, sizeof(int) * ni) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMallocHost maps");
+    if (cudaMalloc(&D->info, sizeof(int) * (2 * MAX_LARGE_COMPONENTS + 2)) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc info");
+    if (cudaMalloc(&D->comp_d, sizeof(long long) * 3 * MAX_LARGE_COMPONENTS) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc comps");
     return ABD_OK;
 }
 
 template <class T>
-static int dense_solve_t(Engine* E, int* iters) {
+static int dense_reserve(Engine* E, DenseState* D, size_t a_elems, size_t rhs_elems, int nmax) {
+    size_t es = sizeof(T);
+    if (a_elems * es > D->A_bytes) {
+        if (D->A) cudaFree(D->A);
+        D->A_bytes = a_elems * es + (a_elems * es) / 4;
+        if (cudaMalloc(&D->A, D->A_bytes) != cudaSuccess) { D->A = nullptr; D->A_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc dense matrices"); }
+    }
+    if (rhs_elems * es > D->rhs_bytes) {
+        if (D->rhs) cudaFree(D->rhs);
+        D->rhs_bytes = rhs_elems * es + 4096;
+        if (cudaMalloc(&D->rhs, D->rhs_bytes) != cudaSuccess) { D->rhs = nullptr; D->rhs_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc dense rhs"); }
+    }
+    if (nmax > D->work_n || D->work_bytes % es) {
+        if (D->work) cudaFree(D->work);
+        if (D->ipiv) cudaFree(D->ipiv);
+        D->work = nullptr; D->ipiv = nullptr;
+        int lw1 = 0, lw2 = 0;
+        if constexpr (sizeof(T) == 4) {
+            cusolverDnSpotrf_bufferSize(D->h, CUBLAS_FILL_MODE_LOWER, nmax, (float*)D->A, nmax, &lw1);
+            cusolverDnSgetrf_bufferSize(D->h, nmax, nmax, (float*)D->A, nmax, &lw2);
+        } else {
+            cusolverDnDpotrf_bufferSize(D->h, CUBLAS_FILL_MODE_LOWER, nmax, (double*)D->A, nmax, &lw1);
+            cusolverDnDgetrf_bufferSize(D->h, nmax, nmax, (double*)D->A, nmax, &lw2);
+        }
+        D->work_bytes = ((size_t)std::max(lw1, lw2) + 32) * es;
+        D->work_n = nmax;
+        if (cudaMalloc(&D->work, D->work_bytes) != cudaSuccess || cudaMalloc(&D->ipiv, sizeof(int) * nmax) != cudaSuccess)
+            return E->fail(ABD_ERR_CUDA, "cudaMalloc cusolver work");
+    }
+    return ABD_OK;
+}
+
+template <class T>
+static cusolverStatus_t potrf(DenseState* D, int n, T* A, T* work, int lwork, int* info) {
+    if constexpr (sizeof(T) == 8) return cusolverDnDpotrf(D->h, CUBLAS_FILL_MODE_LOWER, n, A, n, work, lwork, info);
+    else return cusolverDnSpotrf(D->h, CUBLAS_FILL_MODE_LOWER, n, A, n, work, lwork, info);
+}
+template <class T>
+static cusolverStatus_t potrs(DenseState* D, int n, T* A, T* x, int* info) {
+    if constexpr (sizeof(T) == 8) return cusolverDnDpotrs(D->h, CUBLAS_FILL_MODE_LOWER, n, 1, A, n, x, n, info);
+    else return cusolverDnSpotrs(D->h, CUBLAS_FILL_MODE_LOWER, n, 1, A, n, x, n, info);
+}
+template <class T>
+static cusolverStatus_t lu_solve(DenseState* D, int n, T* A, T* x, T* work, int* info) {
+    cusolverStatus_t cs;
+    if constexpr (sizeof(T) == 8) {
+        cs = cusolverDnDgetrf(D->h, n, n, A, n, work, D->ipiv, info);
+        if (cs == CUSOLVER_STATUS_SUCCESS) cs = cusolverDnDgetrs(D->h, CUBLAS_OP_N, n, 1, A, n, D->ipiv, x, n, info + 1);
+    } else {
+        cs = cusolverDnSgetrf(D->h, n, n, A, n, work, D->ipiv, info);
+        if (cs == CUSOLVER_STATUS_SUCCESS) cs = cusolverDnSgetrs(D->h, CUBLAS_OP_N, n, 1, A, n, D->ipiv, x, n, info + 1);
+    }
+    return cs;
+}
+
+// Returns 1 in *fallback when there are more large components than
+// MAX_LARGE_COMPONENTS or their matrices would exceed 4 GiB (the caller then
+// runs the Krylov solver).
+template <class T>
+static int dense_solve_t(Engine* E, int* iters, int* fallback) {
+    *fallback = 0;
     int rc = dense_init(E);
     if (rc) return rc;
     DenseState* D = ds_of(E);
     cudaStream_t st = E->stream;
     const int* ndone = E->sci + SI_DONE * E->ns;
-    // which scenes still iterate (host copy of the done flags)
-    std::vector<int> done(E->ns);
-    CUDA_TRY(cudaMemcpyAsync(done.data(), ndone, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, st));
+    const int nb = E->nb;
+    // block pattern and done flags to the host
+    const int nk = E->nnzb_host;
+    D->keys.resize(std::max(nk, 1));
+    D->done.resize(E->ns);
+    if (nk > 0) CUDA_TRY(cudaMemcpyAsync(D->keys.data(), E->ukeys, sizeof(unsigned long long) * nk, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(D->done.data(), ndone, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    CUDA_TRY(cudaMemsetAsync(D->A, 0, D->A_bytes, st));
-    T* A = (T*)D->A;
-    k_blocks_to_dense<T><<<grid_for(16L * E->nb), 256, 0, st>>>(E->nb, E->row_ptr, E->bcol, (const T*)E->vals, E->bscene,
-                                                               E->sc_body_begin, D->off_d, ndone, A);
-    T* x = (T*)D->rhs;
-    k_rhs_cast<T><<<grid_for(12L * E->nb), 256, 0, st>>>(12 * E->nb, E->g, x);
-    E->launches += 2;
-    bool projected = E->P.hess_mode == ABD_HESS_PROJECTED;
-    std::vector<int> use_lu(E->ns, projected ? 0 : 1);
-    T* work = (T*)D->work;
-    int lwork = (int)(D->work_bytes / sizeof(T));
-    for (int pass = 0; pass < 2; pass++) {
-        bool any = false;
-        for (int s = 0; s < E->ns; s++) {
-            if (done[s] || D->n[s] == 0) continue;
-            if (pass == 1 && !use_lu[s]) continue;
-            any = true;
-            int n = D->n[s];
-            T* As = A + D->off[s];
-            T* xs = x + 12L * E->h_body_begin[s];
-            cusolverStatus_t cs;
-            if (!use_lu[s]) {
-                if constexpr (sizeof(T) == 8) {
-                    cs = cusolverDnDpotrf(D->h, CUBLAS_FILL_MODE_LOWER, n, (double*)As, n, (double*)work, lwork, D->info);
-                    if (cs == CUSOLVER_STATUS_SUCCESS)
-                        cs = cusolverDnDpotrs(D->h, CUBLAS_FILL_MODE_LOWER, n, 1, (double*)As, n, (double*)xs, n, D->info + 1);
-                } else {
-                    cs = cusolverDnSpotrf(D->h, CUBLAS_FILL_MODE_LOWER, n, (float*)As, n, (float*)work, lwork, D->info);
-                    if (cs == CUSOLVER_STATUS_SUCCESS)
-                        cs = cusolverDnSpotrs(D->h, CUBLAS_FILL_MODE_LOWER, n, 1, (float*)As, n, (float*)xs, n, D->info + 1);
-                }
-                if (cs != CUSOLVER_STATUS_SUCCESS) return E->fail(ABD_ERR_CUDA, "cusolver potrf/potrs");
-                int info = 0;
-                CUDA_TRY(cudaMemcpyAsync(&info, D->info, sizeof(int), cudaMemcpyDeviceToHost, st));
-                CUDA_TRY(cudaStreamSynchronize(st));
-                if (info != 0) use_lu[s] = 1;     // not positive definite: redo with LU in pass 1
+    // union-find over bodies, joined by off-diagonal blocks
+    std::vector<int>& parent = D->parent;
+    parent.resize(nb);
+    for (int b = 0; b < nb; b++) parent[b] = b;
+    auto find = [&](int x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
+    for (int k = 0; k < nk; k++) {
+        unsigned long long key = D->keys[k];
+        if (key == ~0ull) continue;
+        int r = (int)(key / nb), c = (int)(key % nb);
+        if (r == c) continue;
+        int a = find(r), b2 = find(c);
+        if (a != b2) { if (a < b2) parent[b2] = a; else parent[a] = b2; }
+    }
+    D->size.assign(nb, 0);
+    for (int b = 0; b < nb; b++) D->size[find(b)]++;
+    // components of scenes still iterating: small ones (one CTA each) and large ones (cuSOLVER)
+    D->root.assign(nb, -1);
+    D->bmap.assign(nb, -1);
+    std::vector<int> small_root, large_n;
+    std::vector<long long> large_off, large_rhs;
+    long long aoff = 0, roff = 0;
+    int nmax_large = 0, nmax_small = 0, small_bodies = 0;
+    for (int b = 0; b < nb; b++) {
+        int r = find(b), sz = D->size[r];
+        if (sz < 2 || D->done[E->h_bscene[b]]) continue;
+        if (D->root[r] < 0) {
+            if (sz <= SMALL_MAX_BODIES) {
+                D->root[r] = (int)small_root.size();
+                small_root.push_back(r);
+                nmax_small = std::max(nmax_small, 12 * sz);
             } else {
-                if constexpr (sizeof(T) == 8) {
-                    cs = cusolverDnDgetrf(D->h, n, n, (double*)As, n, (double*)work, D->ipiv, D->info);
-                    if (cs == CUSOLVER_STATUS_SUCCESS)
-                        cs = cusolverDnDgetrs(D->h, CUBLAS_OP_N, n, 1, (double*)As, n, D->ipiv, (double*)xs, n, D->info + 1);
-                } else {
-                    cs = cusolverDnSgetrf(D->h, n, n, (float*)As, n, (float*)work, D->ipiv, D->info);
-                    if (cs == CUSOLVER_STATUS_SUCCESS)
-                        cs = cusolverDnSgetrs(D->h, CUBLAS_OP_N, n, 1, (float*)As, n, D->ipiv, (float*)xs, n, D->info + 1);
-                }
-                if (cs != CUSOLVER_STATUS_SUCCESS) return E->fail(ABD_ERR_CUDA, "cusolver getrf/getrs");
+                if ((int)large_n.size() >= MAX_LARGE_COMPONENTS) { *fallback = 1; return ABD_OK; }
+                D->root[r] = (int)large_n.size();
+                int n = 12 * sz;
+                large_n.push_back(n); large_off.push_back(aoff); large_rhs.push_back(roff);
+                aoff += (long long)n * n; roff += n;
+                nmax_large = std::max(nmax_large, n);
             }
         }
-        if (pass == 0) {
-            // scenes that fell back to LU need their matrix and right-hand side again
-            bool redo = false;
-            for (int s = 0; s < E->ns; s++) if (projected && use_lu[s] && !done[s]) redo = true;
-            if (!redo) break;
-            std::vector<int> mask(E->ns, 1);
-            for (int s = 0; s < E->ns; s++) if (use_lu[s] && !done[s]) mask[s] = 0;
-            int* dmask = E->sci + SI_NACT * E->ns;
-            CUDA_TRY(cudaMemcpyAsync(dmask, mask.data(), sizeof(int) * E->ns, cudaMemcpyHostToDevice, st));
-            // right-hand sides of the redone scenes only
-            for (int s = 0; s < E->ns; s++) if (!mask[s]) {
-                int n = D->n[s];
-                CUDA_TRY(cudaMemsetAsync(A + D->off[s], 0, sizeof(T) * (size_t)n * n, st));
-            }
-            k_blocks_to_dense<T><<<grid_for(16L * E->nb), 256, 0, st>>>(E->nb, E->row_ptr, E->bcol, (const T*)E->vals,
-                                                                       E->bscene, E->sc_body_begin, D->off_d, dmask, A);
-            for (int s = 0; s < E->ns; s++) if (!mask[s]) {
-                int n = D->n[s];
-                k_rhs_cast<T><<<grid_for(n), 256, 0, st>>>(n, E->g + 12L * E->h_body_begin[s], x + 12L * E->h_body_begin[s]);
-            }
-            (void)any;
+        if (sz <= SMALL_MAX_BODIES) { D->bmap[b] = -2; small_bodies++; }
+        else D->bmap[b] = D->root[r];
+    }
+    const int nsmall = (int)small_root.size(), nlarge = (int)large_n.size();
+    if (aoff * (long long)sizeof(T) > (4LL << 30)) { *fallback = 1; return ABD_OK; }
+    // local body index inside its component (body order) and the small
+    // components' body lists, packed into one upload
+    int* h = D->imap_h;
+    int* h_bmap = h; int* h_blocal = h + nb; int* h_sptr = h + 2 * nb; int* h_sbody = h_sptr + nsmall + 1;
+    D->fill.assign(nsmall + nlarge, 0);
+    h_sptr[0] = 0;
+    for (int c = 0; c < nsmall; c++) h_sptr[c + 1] = h_sptr[c] + D->size[small_root[c]];
+    for (int b = 0; b < nb; b++) {
+        int m = D->bmap[b];
+        h_bmap[b] = m;
+        h_blocal[b] = 0;
+        if (m == -2) {
+            int c = D->root[find(b)];
+            int l = D->fill[c]++;
+            h_blocal[b] = l;
+            h_sbody[h_sptr[c] + l] = b;
+        } else if (m >= 0) {
+            h_blocal[b] = D->fill[nsmall + m]++;
         }
     }
-    k_rhs_back<T><<<grid_for(12L * E->nb), 256, 0, st>>>(12 * E->nb, x, E->bscene, ndone, E->du);
+    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies;
+    CUDA_TRY(cudaMemcpyAsync(D->imap_d, h, sizeof(int) * nints, cudaMemcpyHostToDevice, st));
+    const int* d_bmap = D->imap_d; const int* d_blocal = D->imap_d + nb;
+    const int* d_sptr = D->imap_d + 2 * nb; const int* d_sbody = d_sptr + nsmall + 1;
+    const bool projected = E->P.hess_mode == ABD_HESS_PROJECTED;
+    if (nsmall > 0) {
+        size_t smem = ((size_t)nmax_small * (nmax_small + 1) + nmax_small) * sizeof(T);
+        if (!D->smem_set[sizeof(T) == 8]) {
+            const size_t nm = 12 * SMALL_MAX_BODIES;
+            CUDA_TRY(cudaFuncSetAttribute(k_small_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)((nm * (nm + 1) + nm) * sizeof(T))));
+            D->smem_set[sizeof(T) == 8] = true;
+        }
+        CUDA_TRY(cudaMemsetAsync(D->info, 0, sizeof(int), st));
+        k_small_solve<T><<<nsmall, SMALL_THREADS, smem, st>>>(nsmall, d_sptr, d_sbody, d_blocal, E->row_ptr, E->bcol,
+                                                              (const T*)E->vals, E->g, projected ? 1 : 0, E->du, D->info);
+        E->launches++;
+    }
+    T* x = nullptr;
+    if (nlarge > 0) {
+        if ((rc = dense_reserve<T>(E, D, (size_t)aoff, (size_t)roff, nmax_large))) return rc;
+        std::vector<long long> comp(3 * nlarge);
+        for (int c = 0; c < nlarge; c++) { comp[c] = large_off[c]; comp[nlarge + c] = large_rhs[c]; comp[2 * nlarge + c] = large_n[c]; }
+        CUDA_TRY(cudaMemcpyAsync(D->comp_d, comp.data(), sizeof(long long) * 3 * nlarge, cudaMemcpyHostToDevice, st));
+        const long long* d_off = D->comp_d; const long long* d_rhs = D->comp_d + nlarge; const long long* d_n = D->comp_d + 2 * nlarge;
+        T* A = (T*)D->A;
+        x = (T*)D->rhs;
+        CUDA_TRY(cudaMemsetAsync(A, 0, sizeof(T) * (size_t)aoff, st));
+        k_blocks_to_dense<T><<<grid_for(16L * nb), 256, 0, st>>>(nb, E->row_ptr, E->bcol, (const T*)E->vals, d_bmap,
+                                                                d_blocal, d_off, d_n, -1, A);
+        k_rhs_gather<T><<<grid_for(12L * nb), 256, 0, st>>>(nb, E->g, d_bmap, d_blocal, d_rhs, x);
+        E->launches += 2;
+        T* work = (T*)D->work;
+        int lwork = (int)(D->work_bytes / sizeof(T));
+        std::vector<char> use_lu(nlarge, projected ? 0 : 1);
+        if (projected) {
+            for (int c = 0; c < nlarge; c++)
+                if (potrf<T>(D, large_n[c], A + large_off[c], work, lwork, D->info + 2 + 2 * c) != CUSOLVER_STATUS_SUCCESS)
+                    return E->fail(ABD_ERR_CUDA, "cusolver potrf");
+            std::vector<int> info(2 * nlarge);
+            CUDA_TRY(cudaMemcpyAsync(info.data(), D->info + 2, sizeof(int) * 2 * nlarge, cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            for (int c = 0; c < nlarge; c++) {
+                if (info[2 * c] != 0) {
+                    // not positive definite after all: rebuild this component for LU
+                    use_lu[c] = 1;
+                    CUDA_TRY(cudaMemsetAsync(A + large_off[c], 0, sizeof(T) * (size_t)large_n[c] * large_n[c], st));
+                    k_blocks_to_dense<T><<<grid_for(16L * nb), 256, 0, st>>>(nb, E->row_ptr, E->bcol, (const T*)E->vals, d_bmap,
+                                                                            d_blocal, d_off, d_n, c, A);
+                    E->launches++;
+                } else if (potrs<T>(D, large_n[c], A + large_off[c], x + large_rhs[c], D->info + 3 + 2 * c) != CUSOLVER_STATUS_SUCCESS) {
+                    return E->fail(ABD_ERR_CUDA, "cusolver potrs");
+                }
+            }
+        }
+        for (int c = 0; c < nlarge; c++)
+            if (use_lu[c] && lu_solve<T>(D, large_n[c], A + large_off[c], x + large_rhs[c], work, D->info + 2 + 2 * c) != CUSOLVER_STATUS_SUCCESS)
+                return E->fail(ABD_ERR_CUDA, "cusolver getrf/getrs");
+    }
+    k_du_scatter<T><<<grid_for(12L * nb), 256, 0, st>>>(nb, E->g, d_bmap, d_blocal, nlarge ? D->comp_d + nlarge : nullptr, x,
+                                                       (const T*)E->dinv, E->bscene, ndone, E->du);
     E->launches++;
     *iters = 1;
     return ABD_OK;
 }
 
-int eng_solve_direct(Engine* E, int* iters) {
-    if (E->mixed) return dense_solve_t<float>(E, iters);
-    return dense_solve_t<double>(E, iters);
+int eng_solve_direct(Engine* E, int* iters, int* fallback) {
+    if (E->mixed) return dense_solve_t<float>(E, iters, fallback);
+    return dense_solve_t<double>(E, iters, fallback);
 }

@@ -107,6 +107,7 @@ struct Engine {
 
     // host-side scene offsets
     std::vector<int> h_body_begin, h_vert_begin, h_edge_begin, h_tri_begin, h_plane_begin;
+    std::vector<int> h_bscene;
 
     // geometry
     double* xbar = nullptr; int* vbody = nullptr; int* vscene = nullptr; int* bscene = nullptr;
@@ -202,7 +203,7 @@ enum {
     SD_COUNT
 };
 // per-scene int slots
-enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_COUNT };
+enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_STALL, SI_COUNT };
 
 // launch helpers
 inline int grid_for(long n, int block = 256) {
@@ -221,7 +222,7 @@ int eng_detect(Engine* E, double filt);               // sorted candidate list a
 int eng_energy(Engine* E, int slot);                   // per-scene energy into scd[slot]
 int eng_assemble(Engine* E);                           // g and blocks at the nxt state (uses the candidate list)
 int eng_solve(Engine* E, int* iters);                  // du = A^-1 g for scenes not done
-int eng_solve_direct(Engine* E, int* iters);           // dense factorization per scene
+int eng_solve_direct(Engine* E, int* iters, int* fallback);   // dense factorization per connected component
 void eng_dense_free(Engine* E);
 long long eng_dense_bytes(Engine* E);
 int eng_ccd(Engine* E, const double* dq, double sign); // per-scene toi into scd[SD_TOI]

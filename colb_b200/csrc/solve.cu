@@ -390,21 +390,22 @@ static int solve_t(Engine* E, int* iters) {
 
 static int resolved_solver(const Engine* E) {
     int kind = E->P.linear_solver;
-    if (kind == ABD_SOLVER_AUTO) {
-        bool fits = E->ns <= 64 && eng_dense_bytes(const_cast<Engine*>(E)) <= (4LL << 30);
-        kind = fits ? ABD_SOLVER_DIRECT : (E->P.hess_mode == ABD_HESS_PROJECTED ? ABD_SOLVER_PCG : ABD_SOLVER_BICGSTAB);
-    }
+    // AUTO: the component-wise direct solve, which itself hands over to the
+    // Krylov solver when a step has too many large components
+    if (kind == ABD_SOLVER_AUTO) kind = ABD_SOLVER_DIRECT;
     return kind;
 }
-bool eng_solver_is_direct(const Engine* E) { return resolved_solver(E) == ABD_SOLVER_DIRECT; }
 
 int eng_solve(Engine* E, int* iters) {
     int kind = resolved_solver(E);
     if (kind == ABD_SOLVER_DIRECT) {
         int ph = phase_begin(E, PH_DENSE);
-        int rc = eng_solve_direct(E, iters);
+        int fallback = 0;
+        int rc = eng_solve_direct(E, iters, &fallback);
         phase_end(E, ph, 0);
-        return rc;
+        if (rc || !fallback) return rc;
+        // too many large components for one factorization each
+        kind = E->P.hess_mode == ABD_HESS_PROJECTED ? ABD_SOLVER_PCG : ABD_SOLVER_BICGSTAB;
     }
     KrylovKind kk(E, kind);
     if (E->mixed) return solve_t<float>(E, iters);

@@ -30,22 +30,22 @@ __global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, cons
 }
 // gauss_newton.py:107-113
 __global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, double min_alpha,
-                            Counters* cnt) {
+                            int* stall, Counters* cnt) {
     __shared__ int pending;
     if (threadIdx.x == 0) pending = 0;
     __syncthreads();
     for (int s = threadIdx.x; s < ns; s += blockDim.x) {
         if (acc[s]) continue;
         if (E1[s] < E0[s]) acc[s] = 1;
-        else if (alpha[s] * 0.5 < min_alpha) acc[s] = 1;
+        else if (alpha[s] * 0.5 < min_alpha) { acc[s] = 1; if (alpha[s] < ABD_LS_STALL_ALPHA) stall[s] = 1; }
         else { alpha[s] *= 0.5; atomicAdd(&pending, 1); }
     }
     __syncthreads();
     if (threadIdx.x == 0) cnt->ls_pending = pending;
 }
 // abd.py:693-699 bookkeeping: record (residual, alpha), stop on tol or cap
-__global__ void k_newton_book(int ns, int* done, int* iter, const double* gg, const double* alpha, double* prof_res,
-                              double* prof_alpha, int max_iter, double tol, Counters* cnt) {
+__global__ void k_newton_book(int ns, int* done, int* iter, const int* stall, const double* gg, const double* alpha,
+                              double* prof_res, double* prof_alpha, int max_iter, double tol, Counters* cnt) {
     __shared__ int ndone, nan;
     if (threadIdx.x == 0) { ndone = 0; nan = 0; }
     __syncthreads();
@@ -57,7 +57,7 @@ __global__ void k_newton_book(int ns, int* done, int* iter, const double* gg, co
             prof_res[(long)s * max_iter + it] = res;
             prof_alpha[(long)s * max_iter + it] = alpha[s];
             iter[s] = it + 1;
-            if (res < tol || it + 1 >= max_iter || !(res == res)) done[s] = 1;
+            if (res < tol || it + 1 >= max_iter || !(res == res) || stall[s]) done[s] = 1;
         }
         if (done[s]) atomicAdd(&ndone, 1);
     }
@@ -116,6 +116,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     int* done = E->sci + SI_DONE * ns;
     int* iter = E->sci + SI_ITER * ns;
     int* acc = E->sci + SI_ACC * ns;
+    int* stall = E->sci + SI_STALL * ns;
     double* alpha = E->scd + SD_ALPHA * ns;
     int mi = P.newton_max_iter;
     double* prof_res = E->prof_d;
@@ -127,6 +128,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     for (int step = 0; step < n_steps; step++) {
         CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int) * ns, s));
         CUDA_TRY(cudaMemsetAsync(iter, 0, sizeof(int) * ns, s));
+        CUDA_TRY(cudaMemsetAsync(stall, 0, sizeof(int) * ns, s));
         CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, sizeof(Counters), s));
         if (P.warm_start == 2) {
             k_ws_inertial<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, P.dt, P.gravity[0], P.gravity[1], P.gravity[2], E->ws);
@@ -184,14 +186,14 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             for (int trial = 0; trial < 64; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
                 { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
-                k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, P.ls_min_alpha, E->dcnt);
+                k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, P.ls_min_alpha, stall, E->dcnt);
                 E->launches += 2;
                 st.ls_trials++;
                 if ((rc = eng_sync_counters(E))) return rc;
                 if (E->hcnt->ls_pending == 0) break;
             }
             phase_end(E, ph_tr, 0);
-            k_newton_book<<<1, 256, 0, s>>>(ns, done, iter, E->scd + SD_GG * ns, alpha, prof_res, prof_alpha, mi,
+            k_newton_book<<<1, 256, 0, s>>>(ns, done, iter, stall, E->scd + SD_GG * ns, alpha, prof_res, prof_alpha, mi,
                                             P.newton_tol, E->dcnt);
             E->launches++;
             if ((rc = eng_sync_counters(E))) return rc;

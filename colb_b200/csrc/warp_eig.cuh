@@ -9,7 +9,8 @@
 // sweep.  A rotation is skipped when |a_pq| is at rounding level against its
 // diagonal pair or against the whole matrix (rank-deficient Hessians drive
 // some diagonals to zero); sweeps stop when none was applied, the same
-// criterion the serial oracle uses.
+// criterion the serial oracle uses.  A matrix whose Cholesky factorization
+// succeeds is left as it is (it is its own projection).
 #pragma once
 #include "common.cuh"
 
@@ -35,7 +36,31 @@ DV void tournament_pair(int m, int r, int k, int& p, int& q) {
     if (p > q) { int t = p; p = q; q = t; }
 }
 
-// Project S.A (n x n, ld 12) in place.  All 32 lanes call it.
+// Cholesky of S.A into S.T (lanes own rows): true when every pivot is
+// positive, i.e. S.A is positive definite and its own PSD projection.
+DV bool warp_is_pd(WarpEigSmem& S, int n) {
+    const int lane = threadIdx.x & 31;
+    for (int e = lane; e < 144; e += 32) S.T[e] = S.A[e];
+    __syncwarp();
+    bool ok = true;
+    for (int k = 0; k < n; k++) {
+        double d = S.T[k*12+k];                 // same value in every lane
+        if (!(d > 0.0)) { ok = false; break; }
+        d = sqrt(d);
+        if (lane > k && lane < n) S.T[lane*12+k] /= d;
+        __syncwarp();
+        if (lane > k && lane < n) {
+            double lik = S.T[lane*12+k];
+            for (int j = k + 1; j <= lane; j++) S.T[lane*12+j] -= lik * S.T[j*12+k];
+        }
+        __syncwarp();
+    }
+    __syncwarp();
+    return ok;
+}
+
+// Project S.A (n x n, ld 12) in place.  All 32 lanes call it.  A positive
+// definite matrix is returned unchanged.
 DV void warp_psd_project(WarpEigSmem& S, int n) {
     const int lane = threadIdx.x & 31;
     const int m = (n & 1) ? n + 1 : n;      // players, index n is a dummy when n is odd
@@ -46,6 +71,7 @@ DV void warp_psd_project(WarpEigSmem& S, int n) {
     for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
     if (fro == 0.0) return;
     __syncwarp();
+    if (warp_is_pd(S, n)) return;
     for (int sweep = 0; sweep < 50; sweep++) {
         if (lane == 0) S.flag = 0;
         __syncwarp();

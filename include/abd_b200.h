@@ -34,6 +34,8 @@ extern "C" {
 #define ABD_ABI_VERSION 1
 
 /* ---- status codes ---------------------------------------------------- */
+#define ABD_LS_STALL_ALPHA 1e-6
+
 #define ABD_OK                   0
 #define ABD_ERR_INVALID_ARG     -1
 #define ABD_ERR_CUDA            -2
@@ -91,7 +93,10 @@ typedef struct AbdParams {
     int32_t newton_max_iter;/* abd.py:679 (16) */
     int32_t ccd;            /* 1: additive-CCD time of impact bounds the line search */
     double ccd_scale;       /* ACCD conservative rescaling s in (0,1) (0.1 typical) */
-    double ls_min_alpha;    /* gauss_newton.py:110: stop halving when alpha*0.5 < this (1e-2) */
+    double ls_min_alpha;    /* gauss_newton.py:110: stop halving when alpha*0.5 < this (1e-2).
+                             * A search that gives up below ABD_LS_STALL_ALPHA
+                             * ends the scene's Newton loop (stalled: the next
+                             * iteration would start from the same state). */
     int32_t precision;      /* ABD_PREC_* */
     int32_t contact_capacity;/* max candidate pairs per detection (reference: 10000, contact.py:8) */
     double pinned_diag;     /* diagonal of pinned bodies' blocks, abd.py:146 (100) */

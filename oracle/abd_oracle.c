@@ -327,10 +327,28 @@ double oracle_pt_dist2(const double p[3], const double a[3], const double b[3], 
 /* ------------------------------------------------------------------ */
 /* Symmetric eigen-decomposition by cyclic Jacobi rotations and the PSD  */
 /* projection V max(L,0) V^T (used where the reference calls            */
-/* x_to_grad_psd_hess_ee, abd.py:247).                                   */
+/* x_to_grad_psd_hess_ee, abd.py:247).  A matrix whose Cholesky         */
+/* factorization succeeds is returned unchanged.                         */
 /* ------------------------------------------------------------------ */
+/* Cholesky without storing the factor: 1 when every pivot is positive, in
+ * which case the matrix is its own PSD projection. */
+static int is_pd(int n, const double* H) {
+    double L[144];
+    memcpy(L, H, (size_t)n * n * sizeof(double));
+    for (int k = 0; k < n; k++) {
+        double d = L[k*n+k];
+        if (!(d > 0)) return 0;
+        d = sqrt(d);
+        for (int i = k + 1; i < n; i++) L[i*n+k] /= d;
+        for (int i = k + 1; i < n; i++)
+            for (int j = k + 1; j <= i; j++) L[i*n+j] -= L[i*n+k] * L[j*n+k];
+    }
+    return 1;
+}
+
 void oracle_psd_project(int n, double* H) {
     double A[144], V[144];
+    if (is_pd(n, H)) return;
     memcpy(A, H, (size_t)n * n * sizeof(double));
     for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) V[i*n+j] = (i == j);
     double fro = 0; for (int i = 0; i < n*n; i++) fro += A[i]*A[i];
@@ -953,6 +971,7 @@ static double vdot(int n, const double* a, const double* b) { double s = 0; for 
 
 static int krylov(const AbdParams* P, const BSR* A, const double* b, double* x, int* iters) {
     int nb = A->nb, n = 12 * nb;
+    if (nb <= 0) { *iters = 0; return 0; }
     double* Dinv = (double*)xalloc(sizeof(double) * 144 * nb);
     for (int r = 0; r < nb; r++) {
         const double* D = NULL;
@@ -961,7 +980,7 @@ static int krylov(const AbdParams* P, const BSR* A, const double* b, double* x, 
     }
     double *r = xalloc(8*n), *p = xalloc(8*n), *v = xalloc(8*n), *y = xalloc(8*n), *s = xalloc(8*n), *z = xalloc(8*n), *t = xalloc(8*n), *rh = xalloc(8*n);
     memset(x, 0, 8*(size_t)n);
-    memcpy(r, b, 8*n);
+    memcpy(r, b, 8*(size_t)n);
     double bn = sqrt(vdot(n, b, b)), tol = P->lin_tol * bn;
     int it = 0, status = 0;
     if (bn == 0) { *iters = 0; goto done; }
@@ -1248,17 +1267,20 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
             if (toi < st->min_toi) st->min_toi = toi;
             if (toi < alpha) alpha = toi;
         }
+        int stalled = 0;
         for (;;) {
             apply_du(S, backup, du, alpha);
             double E1 = scene_energy(w, S, S->st);
             st->ls_trials++;
             if (E1 < E0) break;
-            else if (alpha * 0.5 < P->ls_min_alpha) break;
+            else if (alpha * 0.5 < P->ls_min_alpha) { stalled = alpha < ABD_LS_STALL_ALPHA; break; }
             else alpha *= 0.5;
         }
         it++;
         prof_push(S, res, alpha);
-        if (res < P->newton_tol || it >= P->newton_max_iter) break;
+        /* a search that gave up at a negligible step left the state where it
+         * was: the next iteration would find the same direction */
+        if (res < P->newton_tol || it >= P->newton_max_iter || stalled) break;
     }
     if (!(res < P->newton_tol)) st->unconverged++;
     st->newton_iters += it;

@@ -99,6 +99,37 @@ def test_solve_matches_dense(chain_scene, chain_pairs, solver):
     assert it > 0
 
 
+@pytest.mark.parametrize("hess_mode", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_direct_solve_by_components(chain_scene, chain_pairs, hess_mode, precision):
+    """The direct solver factors each connected component of the contact
+    graph on its own (block inverse, shared-memory factorization for up to
+    12 bodies, cuSOLVER above); the result must equal one dense solve."""
+    eps = 2.2e-16 if precision == 0 else 1.2e-7
+    cases = [(chain_scene, chain_pairs["states"][k]) for k in (1, 2)]
+    net = S.config2_chain_net(n=5, pitch=1.5 - 5e-4, seed=3)
+    cases.append((net, None))
+    for sc, st in cases:
+        if st is None:
+            p = P.config_params(linear_solver=2, hess_mode=hess_mode, precision=precision)
+        else:
+            p = P.reference_params(linear_solver=2, hess_mode=hess_mode, precision=precision)
+        e, o = _pair(p, sc)
+        if st is not None:
+            e.set_state(st); o.set_state(st)
+        du, it = e.solve()
+        g, H = o.assemble()
+        ref = np.linalg.solve(H, g)
+        assert it == 1
+        # backward error of a stable factorization, and the forward error it implies
+        n = len(g)
+        back = np.abs(H @ du - g).max() / (np.abs(H).max() * np.abs(du).max() + np.abs(g).max())
+        assert back <= 10 * n * eps
+        ev = np.abs(np.linalg.eigvalsh(H))
+        cond = ev.max() / ev.min()
+        assert np.abs(du - ref).max() <= max(1e-8, 10 * n * cond * eps) * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("broadphase", [1, 2])
 def test_reference_chain_trajectory(chain_scene, broadphase):
     p = P.reference_params(lin_tol=1e-10, broadphase=broadphase)
