@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
+#include <float.h>
 #include "../../include/abd_b200.h"
 
 // BDFAffine layout (BDF1.py:11-14, quat_util.py:40-47): 48 doubles per body.

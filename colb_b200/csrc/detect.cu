@@ -35,8 +35,8 @@ __global__ void k_transform(int nv, const double* __restrict__ xbar, const int* 
     }
 }
 
-int eng_body_energy(Engine* E, double* Eo, const int* skip);
-int eng_pg_energy(Engine* E, double* Eo, const int* skip);
+int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip);
+int eng_pg_energy(Engine* E, double* Eo, double* En, const int* skip);
 int eng_pg_candidates(Engine* E, double filt);
 
 int eng_transform(Engine* E) {
@@ -399,27 +399,35 @@ int eng_pg_candidates(Engine* E, double filt) {
 // ------------------------------------------------------------------ energies
 __global__ void k_body_energy(int nb, const double* __restrict__ st, const double* __restrict__ mass,
                               const double* __restrict__ J, const int* __restrict__ bscene, double dt,
-                              double g0, double g1, double g2, double k_ortho, const int* done, double* E) {
+                              double g0, double g1, double g2, double k_ortho, const int* done, double* E,
+                              double* En) {
     for (long base = (long)blockIdx.x * blockDim.x; base < nb; base += (long)gridDim.x * blockDim.x) {
         long b = base + threadIdx.x;
         bool valid = b < nb;
         int s = valid ? bscene[b] : 0;
-        double e = 0;
+        double e = 0, en = 0;
         if (valid && !done[s]) {
             const double* now = st + ST_STRIDE * b + ST_NOW; const double* nx = st + ST_STRIDE * b + ST_NXT;
             double eo = ortho_energy(nx + ST_Q, k_ortho);
             double gv[3] = {g0, g1, g2};
-            double n0 = 0, n1 = 0;
+            double n0 = 0, n1 = 0, s0 = 0, s1 = 0;
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 double ct = now[ST_C+k] + dt * now[ST_V+k] + dt * dt * gv[k];
                 double d = nx[ST_C+k] - ct; n0 += d * d;
+                s0 += fabs(d) * (fabs(nx[ST_C+k]) + fabs(ct));
             }
 #pragma unroll
-            for (int r = 0; r < 9; r++) { double d = nx[ST_Q+r] - (now[ST_Q+r] + dt * now[ST_QD+r]); n1 += d * d; }
+            for (int r = 0; r < 9; r++) {
+                double qt = now[ST_Q+r] + dt * now[ST_QD+r];
+                double d = nx[ST_Q+r] - qt; n1 += d * d;
+                s1 += fabs(d) * (fabs(nx[ST_Q+r]) + fabs(qt));
+            }
             e = eo * dt * dt + 0.5 * (n0 * mass[b] + n1 * J[b]);
+            if (En) en = (e + s0 * fabs(mass[b]) + s1 * fabs(J[b]) + dt * dt * ortho_noise(nx + ST_Q, k_ortho)) * DBL_EPSILON;
         } else valid = false;
         warp_reduce_add(E, s, e, valid);
+        if (En) warp_reduce_add(En, s, en, valid);
     }
 }
 
@@ -474,23 +482,26 @@ __global__ void k_pt_energy(int nv, GridView GV, Geo G, const float4* __restrict
     }
 }
 __global__ void k_pg_energy(int nv, Geo G, const int* __restrict__ vscene, double dhat, int barrier, double sc,
-                            const int* done, double* E) {
+                            const int* done, double* E, double* En) {
     for (long base = (long)blockIdx.x * blockDim.x; base < nv; base += (long)gridDim.x * blockDim.x) {
         long v = base + threadIdx.x;
         bool valid = v < nv;
         int s = valid ? vscene[v] : 0;
-        double e = 0;
+        double e = 0, en = 0;
         if (valid && !done[s]) {
             double xh = dhat * dhat;
+            double L = fmax(fabs(G.x[3*v]), fmax(fabs(G.x[3*v+1]), fabs(G.x[3*v+2])));
             for (int pl = G.sc_plane_begin[s]; pl < G.sc_plane_begin[s+1]; pl++) {
                 const double* n = G.planes + 4*pl;
                 double d = n[0] * G.x[3*v] + n[1] * G.x[3*v+1] + n[2] * G.x[3*v+2] - n[3];
                 if (!(d < dhat)) continue;
                 double b0, b1, b2; barrier3(barrier, d * d, xh, b0, b1, b2);
                 e += b0 * sc;
+                en += contact_noise(sc, b0, b1, d * d, fmax(L, fabs(n[3])), 1.0) * DBL_EPSILON;
             }
         } else valid = false;
         warp_reduce_add(E, s, e, valid);
+        if (En) warp_reduce_add(En, s, en, valid);
     }
 }
 
@@ -503,7 +514,7 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
     CUDA_TRY(cudaMemsetAsync(Eo, 0, sizeof(double) * E->ns, s));
     if ((rc = eng_transform(E))) return rc;
     const AbdParams& P = E->P;
-    if ((rc = eng_body_energy(E, Eo, skip))) return rc;
+    if ((rc = eng_body_energy(E, Eo, nullptr, skip))) return rc;
     double sc = P.kappa * P.dt * P.dt;
     Geo G = geo(E);
     if (P.contact_ee && E->ne > 1) {
@@ -526,20 +537,21 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
         phase_end(E, ph, E->nv * (32.0 + 4.0 + 24.0) + E->nt * (12.0 + 32.0 + 4.0 + 4.0) + g.H * 8.0);
         E->launches++;
     }
-    return eng_pg_energy(E, Eo, skip);
+    return eng_pg_energy(E, Eo, nullptr, skip);
 }
-int eng_body_energy(Engine* E, double* Eo, const int* skip) {
+// En (may be null) accumulates the scale of the FP64 evaluation error
+int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip) {
     const AbdParams& P = E->P;
     k_body_energy<<<grid_for(E->nb), 256, 0, E->stream>>>(E->nb, E->st, E->mass, E->J, E->bscene, P.dt, P.gravity[0],
-                                                          P.gravity[1], P.gravity[2], P.k_ortho, skip, Eo);
+                                                          P.gravity[1], P.gravity[2], P.k_ortho, skip, Eo, En);
     E->launches++;
     return ABD_OK;
 }
-int eng_pg_energy(Engine* E, double* Eo, const int* skip) {
+int eng_pg_energy(Engine* E, double* Eo, double* En, const int* skip) {
     const AbdParams& P = E->P;
     if (E->npl > 0) {
         k_pg_energy<<<grid_for(E->nv), 256, 0, E->stream>>>(E->nv, geo(E), E->vscene, P.dhat, P.barrier,
-                                                            P.kappa * P.dt * P.dt, skip, Eo);
+                                                            P.kappa * P.dt * P.dt, skip, Eo, En);
         E->launches++;
     }
     return ABD_OK;

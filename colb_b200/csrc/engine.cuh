@@ -194,7 +194,7 @@ void phase_collect(Engine* E);   // after a stream sync: fold finished records i
 
 // per-scene double slots (scd[slot*ns + s])
 enum {
-    SD_RES = 0, SD_GG, SD_ALPHA, SD_E0, SD_E1, SD_TOI, SD_BB,
+    SD_RES = 0, SD_GG, SD_ALPHA, SD_E0, SD_E1, SD_E0N, SD_E1N, SD_TOI, SD_BB,
     // six Krylov dot-product rings of three slots each
     SD_K0, SD_K1 = SD_K0 + 3, SD_K2 = SD_K1 + 3, SD_K3 = SD_K2 + 3, SD_K4 = SD_K3 + 3, SD_K5 = SD_K4 + 3,
     SD_KS = SD_K5 + 3, SD_KA, SD_KW,   // BiCGSTAB running scalars rho, alpha, omega (even iterations)

@@ -42,6 +42,28 @@ DV double ortho_energy(const double* q, double k) {
         }
     return e * k;
 }
+// Scale of the FP64 evaluation error of ortho_energy (in units of the
+// rounding unit): k sum_ij (t_ij^2 + 4 |t_ij| |a_i| |a_j|), t_ij = a_i.a_j - delta_ij
+DV double ortho_noise(const double* q, double k) {
+    double na[3], e = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) na[i] = sqrt(q[3*i] * q[3*i] + q[3*i+1] * q[3*i+1] + q[3*i+2] * q[3*i+2]);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double t = q[3*i] * q[3*j] + q[3*i+1] * q[3*j+1] + q[3*i+2] * q[3*j+2] - (i == j ? 1.0 : 0.0);
+            e += t * t + 4.0 * fabs(t) * na[i] * na[j];
+        }
+    return e * k;
+}
+// Scale of the FP64 evaluation error of one barrier term sc*b(x), x = d^2,
+// over a stencil whose coordinates are at most L in magnitude: the term
+// itself plus the barrier slope times the error of x from rounded positions
+// (mult scales FP32 distances)
+DV double contact_noise(double sc, double b0, double b1, double x, double L, double mult) {
+    return sc * (fabs(b0) + fabs(b1) * 8.0 * sqrt(fabs(x)) * L * mult);
+}
 DV void ortho_grad(const double* q, double k, double* g) {
 #pragma unroll
     for (int i = 0; i < 3; i++) {

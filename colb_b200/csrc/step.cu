@@ -28,15 +28,16 @@ __global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, cons
         alpha[s] = ccd ? fmin(1.0, toi[s]) : 1.0;
     }
 }
-// gauss_newton.py:107-113
-__global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, double min_alpha,
-                            int* stall, Counters* cnt) {
+// gauss_newton.py:107-113; an energy change within the FP64 evaluation
+// error of the two energies (N0 + N1) is no increase
+__global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, const double* N0,
+                            const double* N1, double min_alpha, int* stall, Counters* cnt) {
     __shared__ int pending;
     if (threadIdx.x == 0) pending = 0;
     __syncthreads();
     for (int s = threadIdx.x; s < ns; s += blockDim.x) {
         if (acc[s]) continue;
-        if (E1[s] < E0[s]) acc[s] = 1;
+        if (E1[s] < E0[s] || E1[s] - E0[s] <= N0[s] + N1[s]) acc[s] = 1;
         else if (alpha[s] * 0.5 < min_alpha) { acc[s] = 1; if (alpha[s] < ABD_LS_STALL_ALPHA) stall[s] = 1; }
         else { alpha[s] *= 0.5; atomicAdd(&pending, 1); }
     }
@@ -186,7 +187,8 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             for (int trial = 0; trial < 64; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
                 { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
-                k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, P.ls_min_alpha, stall, E->dcnt);
+                k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, E->scd + SD_E0N * ns,
+                                              E->scd + SD_E1N * ns, P.ls_min_alpha, stall, E->dcnt);
                 E->launches += 2;
                 st.ls_trials++;
                 if ((rc = eng_sync_counters(E))) return rc;

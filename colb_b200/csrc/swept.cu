@@ -302,12 +302,13 @@ int eng_ccd_list(Engine* E, const int* skip) {
 
 // ------------------------------------------------------------------ energy over the list
 __global__ void k_list_energy(int n, const int4* __restrict__ list, Geo G, const int* __restrict__ bscene,
-                              const int* __restrict__ skip, int f32, double dhat, int barrier, double sc, double* Eo) {
+                              const int* __restrict__ skip, int f32, double dhat, int barrier, double sc, double* Eo,
+                              double* En) {
     for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
         long c = base + threadIdx.x;
         bool valid = c < n;
         int s = 0;
-        double e = 0;
+        double e = 0, en = 0;
         if (valid) {
             int4 C = list[c];
             int v0 = C.x == ABD_CONTACT_EE ? G.edges[C.y].x : C.y;
@@ -318,33 +319,46 @@ __global__ void k_list_energy(int n, const int4* __restrict__ list, Geo G, const
                 if (classify(G, C.x, C.y, C.z, f32, dhat, stv, type, xb)) {
                     double b0, b1, b2; barrier3(barrier, xb, dhat * dhat, b0, b1, b2);
                     e = b0 * sc;
+                    int vs[4] = {stv.x, stv.y, stv.z, stv.w};
+                    double L = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (vs[k] >= 0)
+                            L = fmax(L, fmax(fabs(G.x[3*vs[k]]), fmax(fabs(G.x[3*vs[k]+1]), fabs(G.x[3*vs[k]+2]))));
+                    // FP32 distances carry 2^29 times the FP64 rounding
+                    en = contact_noise(sc, b0, b1, xb, L, (f32 && C.x == ABD_CONTACT_EE) ? 536870912.0 : 1.0) * DBL_EPSILON;
                 }
             }
         }
         warp_reduce_add(Eo, s, e, valid);
+        warp_reduce_add(En, s, en, valid);
     }
 }
 
-int eng_body_energy(Engine* E, double* Eo, const int* skip);
-int eng_pg_energy(Engine* E, double* Eo, const int* skip);
+int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip);
+int eng_pg_energy(Engine* E, double* Eo, double* En, const int* skip);
 
+// energy per scene into scd[slot] and the scale of its FP64 evaluation
+// error into scd[noise slot] (SD_E0 -> SD_E0N, SD_E1 -> SD_E1N)
 int eng_energy_list(Engine* E, int slot, const int* skip) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
     double* Eo = E->scd + slot * E->ns;
+    double* En = E->scd + (slot == SD_E0 ? SD_E0N : SD_E1N) * E->ns;
     CUDA_TRY(cudaMemsetAsync(Eo, 0, sizeof(double) * E->ns, s));
+    CUDA_TRY(cudaMemsetAsync(En, 0, sizeof(double) * E->ns, s));
     int rc = eng_transform(E);
     if (rc) return rc;
-    if ((rc = eng_body_energy(E, Eo, skip))) return rc;
+    if ((rc = eng_body_energy(E, Eo, En, skip))) return rc;
     if (E->n_sw > 0) {
         int ph = phase_begin(E, PH_ELIST);
         k_list_energy<<<grid_for(E->n_sw, 128), 128, 0, s>>>(E->n_sw, E->sw, eng_geo(E), E->bscene, skip, P.ee_f32, P.dhat,
-                                                             P.barrier, P.kappa * P.dt * P.dt, Eo);
+                                                             P.barrier, P.kappa * P.dt * P.dt, Eo, En);
         // per listed pair: the entry, its 2-4 vertex ids and positions
         phase_end(E, ph, E->n_sw * (16.0 + 16.0 + 4 * 24.0));
         E->launches++;
     }
-    return eng_pg_energy(E, Eo, skip);
+    return eng_pg_energy(E, Eo, En, skip);
 }
 
 // ------------------------------------------------------------------ detection from the list

@@ -687,7 +687,7 @@ int oracle_get_pairs(OracleWorld* w, int32_t* out4, int32_t* kinds, int cap, int
 /* One contact: stencil, barrier argument, gradient and Hessian on the  */
 /* stencil points (abd.py:198-571 for EE/PE/PP).                        */
 /* ------------------------------------------------------------------ */
-typedef struct { int n; int v[4]; double e; double g[12]; double H[144]; int active; int type; } CEval;
+typedef struct { int n; int v[4]; double e, noise; double g[12]; double H[144]; int active; int type; } CEval;
 
 #define T_PP 0
 #define T_PE 1
@@ -700,7 +700,7 @@ static void eval_contact(const OracleWorld* w, const OScene* S, const double* x,
     const AbdParams* P = &w->P;
     double xh = P->dhat * P->dhat;
     double sc = P->kappa * P->dt * P->dt;
-    out->active = 0; out->e = 0; out->n = 0;
+    out->active = 0; out->e = 0; out->noise = 0; out->n = 0;
     double xb = 0;  /* barrier argument */
     double f = 0, g[12], H[144], pts[12];
     int type = -1;
@@ -756,6 +756,17 @@ static void eval_contact(const OracleWorld* w, const OScene* S, const double* x,
     double B[3]; oracle_barrier(P->barrier, xb, xh, B);
     out->active = 1; out->type = type;
     out->e = B[0] * sc;
+    {
+        /* scale of the FP64 evaluation error: the term, plus the barrier
+         * slope times the error of x from positions rounded at magnitude L
+         * (FP32 distances carry 2^29 times the FP64 rounding) */
+        double L = 0;
+        for (int k = 0; k < out->n; k++) for (int c = 0; c < 3; c++) L = fmax(L, fabs(x[3*out->v[k] + c]));
+        double mult = 1.0;
+        if (C->kind == ABD_CONTACT_EE && P->ee_f32) mult = 536870912.0;
+        if (C->kind == ABD_CONTACT_PG) L = fmax(L, fabs(S->planes[4*C->b + 3]));
+        out->noise = sc * (fabs(B[0]) + fabs(B[1]) * 8.0 * sqrt(fabs(xb)) * L * mult) * DBL_EPSILON;
+    }
     if (!deriv) return;
     int m = 3 * out->n;
     if (P->hess_mode == ABD_HESS_REFERENCE) {
@@ -776,34 +787,57 @@ static void eval_contact(const OracleWorld* w, const OScene* S, const double* x,
 /* ------------------------------------------------------------------ */
 /* Energy (abd.py:53-75, :725-735)                                       */
 /* ------------------------------------------------------------------ */
-static double body_energy(const OracleWorld* w, const OScene* S, const double* st, int b) {
+/* scale of the FP64 evaluation error of the orthogonality energy:
+ * k sum_ij (t_ij^2 + 4 |t_ij| |a_i| |a_j|), t_ij = a_i.a_j - delta_ij */
+static double ortho_noise(const double q[9], double k) {
+    double na[3], e = 0;
+    for (int i = 0; i < 3; i++) na[i] = sqrt(dot3(q + 3*i, q + 3*i));
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) {
+        double t = dot3(q + 3*i, q + 3*j) - (i == j);
+        e += t * t + 4.0 * fabs(t) * na[i] * na[j];
+    }
+    return e * k;
+}
+/* inertia + orthogonality energy of one body; *noise (may be NULL) gets the
+ * scale of its FP64 evaluation error */
+static double body_energy(const OracleWorld* w, const OScene* S, const double* st, int b, double* noise) {
     const AbdParams* P = &w->P; double dt = P->dt;
     const double* s = st + 48*b;
     const double* now = s + ST_NOW; const double* nx = s + ST_NXT;
     double eo; oracle_ortho(nx + ST_Q, P->k_ortho, &eo, NULL, NULL);
-    double dq0[3], n1 = 0;
+    double dq0[3], n1 = 0, s0 = 0, s1 = 0;
     for (int k = 0; k < 3; k++) {
         double ct = now[ST_C+k] + dt * now[ST_V+k] + dt * dt * P->gravity[k];
         dq0[k] = nx[ST_C+k] - ct;
+        s0 += fabs(dq0[k]) * (fabs(nx[ST_C+k]) + fabs(ct));
     }
-    for (int r = 0; r < 9; r++) { double d = nx[ST_Q+r] - (now[ST_Q+r] + dt * now[ST_QD+r]); n1 += d * d; }
+    for (int r = 0; r < 9; r++) {
+        double qt = now[ST_Q+r] + dt * now[ST_QD+r];
+        double d = nx[ST_Q+r] - qt; n1 += d * d;
+        s1 += fabs(d) * (fabs(nx[ST_Q+r]) + fabs(qt));
+    }
     double nm = dot3(dq0, dq0) * S->mass[b] + n1 * S->J[b];
-    return eo * dt * dt + 0.5 * nm;
+    double e = eo * dt * dt + 0.5 * nm;
+    if (noise) *noise = (e + s0 * fabs(S->mass[b]) + s1 * fabs(S->J[b]) + dt * dt * ortho_noise(nx + ST_Q, P->k_ortho)) * DBL_EPSILON;
+    return e;
 }
-static double scene_energy(const OracleWorld* w, OScene* S, const double* st) {
-    double e = 0;
-    for (int b = 0; b < S->nb; b++) e += body_energy(w, S, st, b);
+/* total energy of a scene; *noise (may be NULL) gets the scale of its FP64
+ * evaluation error (sum over terms) */
+static double scene_energy(const OracleWorld* w, OScene* S, const double* st, double* noise) {
+    double e = 0, en = 0;
+    for (int b = 0; b < S->nb; b++) { double nb_; e += body_energy(w, S, st, b, &nb_); en += nb_; }
     transform(S, st, S->x);
     detect(w, S, S->x, w->P.cand_dist);   /* abd.py:732: re-detect with the candidate filter */
-    double* ec = (double*)xalloc(sizeof(double) * (S->nc + 1));
+    double* ec = (double*)xalloc(sizeof(double) * 2 * (S->nc + 1));
     #pragma omp parallel for num_threads(g_threads) schedule(dynamic, 64)
-    for (int c = 0; c < S->nc; c++) { CEval ce; eval_contact(w, S, S->x, &S->cand[c], 0, &ce); ec[c] = ce.e; }
-    for (int c = 0; c < S->nc; c++) e += ec[c];
+    for (int c = 0; c < S->nc; c++) { CEval ce; eval_contact(w, S, S->x, &S->cand[c], 0, &ce); ec[2*c] = ce.e; ec[2*c+1] = ce.noise; }
+    for (int c = 0; c < S->nc; c++) { e += ec[2*c]; en += ec[2*c+1]; }
     free(ec);
+    if (noise) *noise = en;
     return e;
 }
 int oracle_energy(OracleWorld* w, double* e) {
-    for (int i = 0; i < w->ns; i++) e[i] = scene_energy(w, &w->s[i], w->s[i].st);
+    for (int i = 0; i < w->ns; i++) e[i] = scene_energy(w, &w->s[i], w->s[i].st, NULL);
     return 0;
 }
 
@@ -1258,7 +1292,8 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
         free(as.g); bsr_free(&as.A);
         /* line search */
         memcpy(backup, S->st, sizeof(double) * 48 * nb);
-        double E0 = scene_energy(w, S, S->st);
+        double N0, N1;
+        double E0 = scene_energy(w, S, S->st, &N0);
         double alpha = 1.0;
         if (P->ccd) {
             transform(S, S->st, S->x);
@@ -1270,9 +1305,10 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
         int stalled = 0;
         for (;;) {
             apply_du(S, backup, du, alpha);
-            double E1 = scene_energy(w, S, S->st);
+            double E1 = scene_energy(w, S, S->st, &N1);
             st->ls_trials++;
-            if (E1 < E0) break;
+            /* a change within the FP64 evaluation error of both energies is no increase */
+            if (E1 < E0 || E1 - E0 <= N0 + N1) break;
             else if (alpha * 0.5 < P->ls_min_alpha) { stalled = alpha < ABD_LS_STALL_ALPHA; break; }
             else alpha *= 0.5;
         }
