@@ -142,6 +142,8 @@ int eng_alloc(Engine* E) {
 
 void eng_free(Engine* E) {
     eng_dense_free(E);
+    eng_features_free(E);
+    eng_mlp_free(E);
     eng_bp_free(E);
     void* bd[] = {E->bd_vbeg, E->bd_ebeg, E->bd_tbeg};
     for (void* p : bd) if (p) cudaFree(p);
@@ -257,6 +259,7 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     E->h_edges = edges; E->h_tris = tris;
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) { delete E; g_err = "stream"; return ABD_ERR_CUDA; }
     if (P.broadphase < 0 || P.broadphase > 2) { delete E; g_err = "abd_create: broadphase must be 0, 1 or 2"; return ABD_ERR_INVALID_ARG; }
+    if (P.warm_start < 0 || P.warm_start > 3) { delete E; g_err = "abd_create: warm_start must be 0..3"; return ABD_ERR_INVALID_ARG; }
     auto up = [&](auto*& dst, auto& src) -> int {
         using T = typename std::remove_reference<decltype(src)>::type::value_type;
         int rc = dalloc(E, (T**)&dst, src.size());

@@ -161,6 +161,8 @@ struct Engine {
 
     double* prof_d = nullptr;      // [2][ns][newton_max_iter] residual / alpha of the current step
     void* dense_state = nullptr;   // direct-solver state (dense.cu)
+    void* feat_state = nullptr;    // feature records (features.cu)
+    void* mlp = nullptr;           // learned warm start network (mlp.cu)
     void* bp_state = nullptr;      // body-pair broad phase scratch (bpair.cu)
     bool bd_ok = false;            // bodies own contiguous vertex / edge / triangle ranges
     int* bd_vbeg = nullptr; int* bd_ebeg = nullptr; int* bd_tbeg = nullptr;   // [nb+1]
@@ -224,6 +226,10 @@ int eng_assemble(Engine* E);                           // g and blocks at the nx
 int eng_solve(Engine* E, int* iters);                  // du = A^-1 g for scenes not done
 int eng_solve_direct(Engine* E, int* iters, int* fallback);   // dense factorization per connected component
 void eng_dense_free(Engine* E);
+void eng_features_free(Engine* E);
+void eng_mlp_free(Engine* E);
+int eng_features(Engine* E, float* feat_dev);     // per-body features at the nxt state
+int eng_learned_ws(Engine* E);                     // network increment into ws
 long long eng_dense_bytes(Engine* E);
 int eng_ccd(Engine* E, const double* dq, double sign); // per-scene toi into scd[SD_TOI]
 int eng_step(Engine* E, int n_steps, AbdStepStats* stats);

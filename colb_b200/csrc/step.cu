@@ -135,6 +135,9 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             k_ws_inertial<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, P.dt, P.gravity[0], P.gravity[1], P.gravity[2], E->ws);
             E->launches++;
             E->has_ws = 1;
+        } else if (P.warm_start == 3) {
+            if ((rc = eng_learned_ws(E))) return rc;
+            E->has_ws = 1;
         }
         if (E->has_ws) {
             // warm start: list and CCD along now -> now + ws, then move

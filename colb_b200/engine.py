@@ -21,8 +21,10 @@ EXPORTS = [
     "abd_step", "abd_get_profile", "abd_get_vertices", "abd_get_pairs", "abd_get_contact_points",
     "abd_energy", "abd_assemble", "abd_solve", "abd_set_warm_start", "abd_get_features",
     "abd_count_intersections", "abd_last_error", "abd_abi_version", "abd_set_timing", "abd_get_timing",
-    "abd_ee_pairs_static",
+    "abd_ee_pairs_static", "abd_set_mlp", "abd_mlp_forward", "abd_trainer_create", "abd_trainer_destroy",
+    "abd_trainer_last_error", "abd_trainer_set_data", "abd_trainer_epoch", "abd_trainer_grad", "abd_trainer_params",
 ]
+MLP_IN, MLP_OUT, MLP_NPARAM, MLP_NNORM = 48, 12, 147212, 120
 PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv", "asm_keys", "asm_body",
           "asm_contact", "asm_inverse", "dense", "swept", "energy_list", "ls_trials"]
 
@@ -66,6 +68,16 @@ def load_library(path=LIB_PATH):
     L.abd_set_timing.argtypes = [vp, C.c_int32, C.c_int32]
     L.abd_get_timing.argtypes = [vp, dp, C.POINTER(C.c_int64), dp]
     L.abd_ee_pairs_static.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_double, vp, C.c_int32, vp, vp]
+    L.abd_set_mlp.argtypes = [vp, fp, fp]
+    L.abd_mlp_forward.argtypes = [vp, fp, C.c_int32, fp]
+    L.abd_trainer_create.argtypes = [C.c_int32, fp, C.POINTER(vp)]
+    L.abd_trainer_destroy.argtypes = [vp]
+    L.abd_trainer_last_error.argtypes = [vp]
+    L.abd_trainer_last_error.restype = C.c_char_p
+    L.abd_trainer_set_data.argtypes = [vp, fp, fp, C.c_int32]
+    L.abd_trainer_epoch.argtypes = [vp, ip, C.c_int32, C.c_int32, C.c_float, fp]
+    L.abd_trainer_grad.argtypes = [vp, fp, fp, C.c_int32, fp, fp]
+    L.abd_trainer_params.argtypes = [vp, fp]
     _lib = L
     return L
 
@@ -82,6 +94,15 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a if shape is None else a.reshape(shape)
 
 
 class Engine:
@@ -178,6 +199,18 @@ class Engine:
         dq = np.ascontiguousarray(dq, dtype=np.float32).reshape(self.nb, 12)
         self._check(self.L.abd_set_warm_start(self.h, dq.ctypes.data_as(C.POINTER(C.c_float)), self.nb))
 
+    def set_mlp(self, params, norm):
+        """Network of the learned warm start (warm_start 3): ABD_MLP_NPARAM
+        parameters and ABD_MLP_NNORM normalisation floats."""
+        params = _f32(params, (MLP_NPARAM,)); norm = _f32(norm, (MLP_NNORM,))
+        self._check(self.L.abd_set_mlp(self.h, _fp(params), _fp(norm)))
+
+    def mlp_forward(self, x):
+        x = _f32(x).reshape(-1, MLP_IN)
+        y = np.zeros((len(x), MLP_OUT), dtype=np.float32)
+        self._check(self.L.abd_mlp_forward(self.h, _fp(x), len(x), _fp(y)))
+        return y
+
     def features(self):
         f = np.zeros((self.nb, 48), dtype=np.float32)
         self._check(self.L.abd_get_features(self.h, f.ctypes.data_as(C.POINTER(C.c_float)), self.nb))
@@ -195,3 +228,55 @@ class Engine:
         n = C.c_int32()
         self._check(self.L.abd_count_intersections(self.h, C.byref(n)))
         return n.value
+
+
+class Trainer:
+    """GPU trainer of the warm-start network (abd_trainer_*)."""
+
+    def __init__(self, params, device=0):
+        self.L = load_library()
+        h = C.c_void_p()
+        params = _f32(params, (MLP_NPARAM,))
+        rc = self.L.abd_trainer_create(device, _fp(params), C.byref(h))
+        self.h = h
+        if rc != ABD_OK:
+            msg = self.L.abd_trainer_last_error(h).decode() if h.value else "no device"
+            self.close()
+            raise AbdError(rc, msg)
+
+    def _check(self, rc):
+        if rc != ABD_OK:
+            raise AbdError(rc, self.L.abd_trainer_last_error(self.h).decode())
+
+    def set_data(self, x, y):
+        x = _f32(x).reshape(-1, MLP_IN); y = _f32(y).reshape(-1, MLP_OUT)
+        self._check(self.L.abd_trainer_set_data(self.h, _fp(x), _fp(y), len(x)))
+
+    def epoch(self, order, batch, lr):
+        order = np.ascontiguousarray(order, dtype=np.int32)
+        loss = C.c_float()
+        self._check(self.L.abd_trainer_epoch(self.h, _ip(order), len(order), batch, lr, C.byref(loss)))
+        return loss.value
+
+    def grad(self, x, y):
+        x = _f32(x).reshape(-1, MLP_IN); y = _f32(y).reshape(-1, MLP_OUT)
+        g = np.zeros(MLP_NPARAM, dtype=np.float32)
+        loss = C.c_float()
+        self._check(self.L.abd_trainer_grad(self.h, _fp(x), _fp(y), len(x), _fp(g), C.byref(loss)))
+        return loss.value, g
+
+    def params(self):
+        p = np.zeros(MLP_NPARAM, dtype=np.float32)
+        self._check(self.L.abd_trainer_params(self.h, _fp(p)))
+        return p
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.abd_trainer_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -103,7 +103,8 @@ typedef struct AbdParams {
     int32_t warm_start;     /* 0: start Newton from nxt = now (abd.py: history.nxt == now after
                                forward_states); 1: from now + the increment given to
                                abd_set_warm_start; 2: from the inertial prediction
-                               (c + dt v + dt^2 g, q + dt qdot); 1 and 2 are clipped by CCD */
+                               (c + dt v + dt^2 g, q + dt qdot); 3: from the learned network
+                               (abd_set_mlp); 1, 2 and 3 are clipped by CCD */
     int32_t broadphase;     /* 0 auto, 1 hashed grid over primitives, 2 body pairs then primitives
                                (needs contiguous per-body vertex/edge/triangle ranges) */
     int32_t reserved[6];
@@ -217,9 +218,53 @@ int abd_solve(AbdHandle* h, double* du, int32_t* iters);
  * Values are in DoF order [c, q0, q1, q2]; the increment is clipped by CCD. */
 int abd_set_warm_start(AbdHandle* h, const float* dq12, int32_t n_bodies);
 
-/* Per-body features for the learned warm start: 48 floats per body
- * (q 9, qdot 9, q_tilde 12, contact count 1, 8 smallest contact distances ... ). */
+/* Learned warm start (no reference counterpart).
+ *
+ * Features: 48 floats per body at the current state, in the body frame
+ * (a direction d maps to q d, q the body's 3x3 DoF rows):
+ *   [0:3]   q (v + dt g)          [3:12] q qdot^T (row-major)
+ *   [12:15] q g / |g|             [15]   log(1 + number of nearby pairs)
+ *   [16 + 4k] distance / radius, [17 + 4k : 20 + 4k] unit direction from the
+ *   other primitive, for the 8 nearest pairs (missing ones: 1, 0, 0, 0);
+ *   pairs are those within radius = ABD_FEAT_RADIUS_DHAT * dhat; pinned
+ *   bodies get zeros.
+ * Network: 48 -> 256 -> 256 -> 256 -> 12, GELU, BF16 weights and
+ * activations, FP32 accumulation.  Parameters are ABD_MLP_NPARAM floats:
+ * W1[256][48] b1[256] W2[256][256] b2[256] W3[256][256] b3[256] W4[12][256]
+ * b4[12]; normalisation is ABD_MLP_NNORM floats: x mean[48], x std[48],
+ * y mean[12], y std[12].  The output y (12) is the body-frame correction
+ * to the inertial increment, per unit time:
+ *   dc = dt v + dt^2 g + dt q^-1 y[0:3]
+ *   dq = dt qdot + dt (q^-1 Y)^T, Y = y[3:12] as a row-major 3x3. */
+#define ABD_FEAT_RADIUS_DHAT 50.0
+#define ABD_MLP_IN 48
+#define ABD_MLP_HIDDEN 256
+#define ABD_MLP_OUT 12
+#define ABD_MLP_NPARAM 147212
+#define ABD_MLP_NNORM 120
 int abd_get_features(AbdHandle* h, float* feat_out, int32_t n_bodies);
+
+/* Sets the network used by warm_start 3 (copied and packed to BF16). */
+int abd_set_mlp(AbdHandle* h, const float* params, const float* norm);
+
+/* The network on n host rows of raw features -> n x 12 outputs (y above);
+ * runs the same tensor-core kernel as warm_start 3. */
+int abd_mlp_forward(AbdHandle* h, const float* x, int32_t n, float* y);
+
+/* Trainer of the network on one GPU: FP32 master weights, Adam (0.9, 0.999,
+ * 1e-8), mean-squared error on normalised targets, forward with BF16-rounded
+ * weights and activations like inference. */
+typedef struct AbdTrainer AbdTrainer;
+int abd_trainer_create(int32_t device, const float* params, AbdTrainer** out);
+int abd_trainer_destroy(AbdTrainer* t);
+const char* abd_trainer_last_error(AbdTrainer* t);
+/* x: n x 48 normalised features, y: n x 12 normalised targets (copied). */
+int abd_trainer_set_data(AbdTrainer* t, const float* x, const float* y, int32_t n);
+/* One pass over order[0..n) in mini-batches, one Adam step each. */
+int abd_trainer_epoch(AbdTrainer* t, const int32_t* order, int32_t n, int32_t batch, float lr, float* mean_loss);
+/* Loss and gradient (ABD_MLP_NPARAM floats) on the given rows, no update. */
+int abd_trainer_grad(AbdTrainer* t, const float* x, const float* y, int32_t n, float* grad, float* loss);
+int abd_trainer_params(AbdTrainer* t, float* params);
 
 /* Number of edge-triangle intersections between different bodies at the
  * nxt state (FP64 exact predicate); 0 means intersection-free. */
