@@ -77,6 +77,24 @@ __global__ void k_forward(int nb, double* st, double dt) {
         for (int k = 0; k < 24; k++) s[ST_NOW + k] = s[ST_NXT + k];
     }
 }
+// warm start as a line-search direction: du = -ws on dynamic bodies
+__global__ void k_ws_to_du(int nb, const double* __restrict__ ws, const double* __restrict__ mass, double* du) {
+    GS_LOOP(i, 12L * nb) du[i] = mass[i / 12] > 0.0 ? -ws[i] : 0.0;
+}
+// accept a warm start that lowers the energy below that of now; after the
+// last trial the scene starts from now (alpha 0, applied once more)
+__global__ void k_ws_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, int last, Counters* cnt) {
+    __shared__ int pending;
+    if (threadIdx.x == 0) pending = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        if (acc[s]) continue;
+        if (E1[s] < E0[s]) acc[s] = 1;
+        else { alpha[s] = last ? 0.0 : alpha[s] * 0.5; atomicAdd(&pending, 1); }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cnt->ls_pending = pending;
+}
 // inertial prediction as an increment from now: ws = q_tilde - q_now
 __global__ void k_ws_inertial(int nb, const double* __restrict__ st, double dt, double g0, double g1, double g2,
                               double* ws) {
@@ -87,17 +105,6 @@ __global__ void k_ws_inertial(int nb, const double* __restrict__ st, double dt, 
         ws[i] = k < 3 ? dt * now[ST_V + k] + dt * dt * gv : dt * now[ST_QD + (k - 3)];
     }
 }
-// warm start: nxt = now + a * ws (dynamic bodies), a = min(1, toi) per scene
-__global__ void k_ws_apply(int nb, double* st, const double* __restrict__ ws, const double* __restrict__ toi,
-                           const int* __restrict__ bscene, const double* __restrict__ mass, int ccd) {
-    GS_LOOP(i, 12L * nb) {
-        long b = i / 12;
-        if (!(mass[b] > 0.0)) continue;
-        double a = ccd ? fmin(1.0, toi[bscene[b]]) : 1.0;
-        st[ST_STRIDE * b + ST_NXT + (i % 12)] = st[ST_STRIDE * b + ST_NOW + (i % 12)] + a * ws[i];
-    }
-}
-
 int eng_grow_contacts(Engine* E, int need);
 
 // algorithmic bytes of one detection: positions in, float copy out, per
@@ -140,11 +147,26 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             E->has_ws = 1;
         }
         if (E->has_ws) {
-            // warm start: list and CCD along now -> now + ws, then move
+            // warm start: list and CCD along now -> now + ws, then move to
+            // now + a ws, a = min(1, toi) halved until the energy is below
+            // that of now (at most 7 halvings, else a = 0)
             if ((rc = eng_swept(E, E->ws, 1.0, done))) return rc;
             if (P.ccd && (rc = eng_ccd_list(E, done))) return rc;
-            k_ws_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->ws, E->scd + SD_TOI * ns, E->bscene, E->mass, P.ccd);
-            E->launches++;
+            k_ws_to_du<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->ws, E->mass, E->du);
+            k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
+            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
+            E->launches += 3;
+            if ((rc = eng_energy_list(E, SD_E0, done))) return rc;
+            for (int trial = 0;; trial++) {
+                k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
+                E->launches++;
+                if (trial == 8) break;
+                if ((rc = eng_energy_list(E, SD_E1, acc))) return rc;
+                k_ws_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, trial == 7, E->dcnt);
+                E->launches++;
+                if ((rc = eng_sync_counters(E))) return rc;
+                if (E->hcnt->ls_pending == 0) break;
+            }
             E->has_ws = 0;
         }
         for (int it = 0; it < mi; it++) {

@@ -1279,7 +1279,17 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
         for (int b = 0; b < nb; b++) if (!dynamic(S, b)) memset(du + 12*b, 0, 96);
         double a = 1.0;
         if (P->ccd) { transform(S, S->st, S->x); vertex_disp(S, du, -1.0, pv); a = scene_ccd(w, S, S->x, pv); }
-        apply_du(S, backup, du, a);
+        /* keep the start only where it lowers the energy below that of now
+         * (nxt == now here): halve at most 7 times, else start from now */
+        double E0 = scene_energy(w, S, S->st, NULL);
+        int ok = 0;
+        for (int t = 0; t < 8; t++) {
+            apply_du(S, backup, du, a);
+            double E1 = scene_energy(w, S, S->st, NULL);
+            if (E1 < E0) { ok = 1; break; }
+            a *= 0.5;
+        }
+        if (!ok) apply_du(S, backup, du, 0.0);
         S->has_ws = 0;
     }
     int it = 0;

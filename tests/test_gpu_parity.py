@@ -155,6 +155,24 @@ def test_config_cubes_trajectory_and_no_intersection(broadphase):
         assert e.count_intersections() == 0
 
 
+@pytest.mark.parametrize("warm_start", [1, 2])
+def test_warm_start_trajectory_matches_oracle(warm_start):
+    """Inertial (2) and user (1) warm starts: CCD-clipped, halved until the
+    energy drops below that of now, then the same Newton loop."""
+    sc = S.config1_cubes(seed=4)
+    p = P.config_params(lin_tol=1e-10, warm_start=warm_start)
+    e, o = _pair(p, sc)
+    rng = np.random.default_rng(1)
+    for _ in range(6):
+        if warm_start == 1:
+            dq = rng.normal(scale=1e-3, size=(e.nb, 12)).astype(np.float32)
+            e.set_warm_start(dq); o.set_warm_start(dq)
+        e.step(2 if warm_start == 2 else 1); o.step(2 if warm_start == 2 else 1)
+        xe, xo = e.vertices(), o.vertices()
+        assert np.abs(xe - xo).max() <= 1e-6 * np.abs(xo).max()
+        assert e.count_intersections() == 0
+
+
 def test_batch_equals_single_scenes():
     scenes = S.config3_batch(n_scenes=4, seed=7, nmin=4, nmax=8)
     p = P.config_params(lin_tol=1e-10)
