@@ -40,11 +40,14 @@ METRIC = "ABD body-steps/s @1e-5 residual: learned+batched vs plain, same B200; 
 def make_workload(name, rank=0, precision=0, ns_batch=512):
     from colb_b200 import params as P, scene as S
     if name == "net16":
-        sc = S.config2_chain_net(n=16, seed=rank)
+        from colb_b200 import fixtures
+        state, t0, seed = fixtures.load_net16()
+        sc = dict(S.config2_chain_net(n=16, seed=seed), state=state)
         p = P.config_params(dt=1.0 / 240.0, precision=precision)
-        cfg = dict(workload="net16: 16x16 torus chain mail, 256 links (R 1.0, r 0.25, 24x12 -> 288 v / 576 t), "
-                   "4 corners pinned, dt 1/240, log barrier dhat 1e-3 kappa 1e7, k_ortho 1e7, CCD line search",
-                   bodies=256, verts=len(sc["xbar"]), tris=len(sc["tris"]))
+        cfg = dict(workload=f"net16: 16x16 torus chain mail, 256 links (R 1.0, r 0.25, 24x12 -> 288 v / 576 t), "
+                   f"4 corners pinned, dt 1/240, log barrier dhat 1e-3 kappa 1e7, k_ortho 1e7, CCD line search; "
+                   f"timed from the resting state after {t0} plain FP64 steps (colb_b200/data/net16_t120.npz)",
+                   bodies=256, verts=len(sc["xbar"]), tris=len(sc["tris"]), start_step=t0)
         return [sc], p, cfg
     if name == "net16c":
         sc = S.config2_chain_net(n=16, seed=rank, pitch=1.5 - 5e-4)
@@ -231,6 +234,41 @@ def run_ours(args, rank, world):
                 bytes_state=48 * 8 * eng.nb)
 
 
+def run_forms(args, scenes, p, dev=0):
+    """The three forms beside the plain FP64 solver on the same workload:
+    mixed precision, the learned warm start, and 8 scenes batched in one
+    handle (alone and all together).  Device time of min(K, 10) steps after
+    2 warm-up steps, from the same start state."""
+    import torch
+    from colb_b200 import learned as Lr
+    from colb_b200._abi import params_to_dict, params_from_dict
+    from colb_b200.engine import Engine
+    params, norm, meta = Lr.load()
+    steps = max(1, min(args.steps, 10))
+    base = params_to_dict(p)
+    forms = {"mixed": (dict(precision=1), 1, False), "learned": (dict(warm_start=3), 1, True),
+             "batched_x8": ({}, 8, False), "learned+batched_x8+mixed": (dict(precision=1, warm_start=3), 8, True)}
+    out = {}
+    for name, (over, copies, learned) in forms.items():
+        e = Engine(params_from_dict(dict(base, **over)), list(scenes) * copies, device=dev)
+        if learned:
+            e.set_mlp(params, norm)
+        nb = dynamic_bodies(scenes) * copies
+        for _ in range(2):
+            e.step(1, allow=(-6, -7))
+        torch.cuda.synchronize()
+        ms = it = unconv = 0
+        for _ in range(steps):
+            rc, st = e.step(1, allow=(-6, -7))
+            ms += st.gpu_ms; it += st.newton_iters; unconv += st.unconverged
+        out[name] = {"value": nb * steps / (ms / 1000.0), "unit": "body-steps/s",
+                     "newton_iters_per_step": it / (steps * len(scenes) * copies), "unconverged_steps": unconv,
+                     "steps": steps, "intersections": e.count_intersections()}
+        e.close()
+    out["learned_model"] = dict(meta, file="colb_b200/data/warmstart_net16.npz")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -240,6 +278,7 @@ def main():
     ap.add_argument("--workload", default="net16", choices=["net16", "net16c", "chain", "cubes", "batch"])
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed FP32/FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed / learned / batched measurements")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -298,6 +337,11 @@ def main():
         "phases_ms_per_step": {k: v["ms"] / r["n_timing"] for k, v in ph.items()},
         "clocks": r["clocks"],
     }
+    if rank == 0 and world == 1 and args.workload == "net16" and not args.no_forms:
+        forms = {"plain_fp64": {"value": value, "unit": "body-steps/s",
+                                "newton_iters_per_step": line["newton_iters_per_step"], "steps": args.steps}}
+        forms.update(run_forms(args, r["scenes"], r["p"]))
+        line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(r["scenes"], r["p"], r["cfg"])
     if rank == 0:

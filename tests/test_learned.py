@@ -123,3 +123,32 @@ def test_features_match_oracle(which):
             tied = np.sum(np.abs(d_ref[b] - d_ref[b, k]) < 1e-6) > 1
             if not tied:
                 assert np.allclose(f[b, 17 + 4 * k:20 + 4 * k], ref[b, 17 + 4 * k:20 + 4 * k], atol=1e-5), (b, k)
+
+
+@pytest.mark.gpu
+def test_trained_network_gain_over_plain(capsys):
+    """What the shipped network (trained on other chain nets) changes on an
+    unseen one: Newton iterations per step of warm_start 3 against the plain
+    start.  Both must reach the residual every step with no intersection;
+    the ratio is measured and printed, not assumed."""
+    from colb_b200 import learned as Lr, params as P, scene as S
+    from colb_b200.engine import Engine
+    params, norm, _ = Lr.load()
+    sc = S.config2_chain_net(n=8, seed=123)
+    iters = {}
+    for ws in (0, 3):
+        e = Engine(P.config_params(dt=1.0 / 240.0, warm_start=ws), sc)
+        if ws == 3:
+            e.set_mlp(params, norm)
+        tot = unconv = 0
+        for _ in range(40):
+            rc, st = e.step(1, allow=(-7,))
+            tot += st.newton_iters
+            unconv += st.unconverged
+        assert unconv == 0
+        assert e.count_intersections() == 0
+        iters[ws] = tot / 40
+    with capsys.disabled():
+        print(f"\nlearned warm start: {iters[3]:.2f} Newton iterations/step vs {iters[0]:.2f} plain "
+              f"(ratio {iters[3] / iters[0]:.2f})")
+    assert iters[3] > 0 and iters[0] > 0
