@@ -81,28 +81,55 @@ def dynamic_bodies(scenes):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """SM clocks and clock-event (throttle) reasons while the timed region
+    runs, read in-process through NVML every 0.25 s (reading only; spawning
+    nvidia-smi instead stalls the host-synchronous step loop).  Falls back to
+    nvidia-smi when NVML cannot be loaded."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device=0):
+    def __init__(self, device=0, period=0.25):
         self.device = device
-        self.rows = []
+        self.period = period
+        self.rows = []           # (sm_mhz, sm_max_mhz, reasons bitmask)
         self._stop = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
+        self._nv = None
+
+    def _sample_nvml(self, h):
+        nv = self._nv
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.rows.append((float(sm), float(mx), int(rs)))
+
+    def _sample_smi(self):
+        fields = "clocks.sm,clocks.max.sm,clocks_event_reasons.active"
+        out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + fields,
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        if out.returncode == 0 and out.stdout.strip():
+            c = [x.strip() for x in out.stdout.strip().split(",")]
+            self.rows.append((float(c[0]), float(c[1]), int(c[2], 16)))
 
     def _run(self):
+        h = None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self._nv = nv
+            h = nv.nvmlDeviceGetHandleByIndex(self.device)
+        except Exception:
+            self._nv = None
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+                if self._nv is not None:
+                    self._sample_nvml(h)
+                else:
+                    self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(self.period)
 
     def __enter__(self):
         self._t.start()
@@ -114,13 +141,11 @@ class ClockSampler:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
+        bits = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+        reasons = sorted({name for r in self.rows for name, bit in bits.items() if r[2] & bit})
+        return {"sm_mhz": float(np.median([r[0] for r in self.rows])), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml" if self._nv is not None else "nvidia-smi"}
 
 
 def measured_peaks():
@@ -176,7 +201,14 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     scenes, p, cfg = make_workload(args.workload, rank, args.precision)
+    if args.warm_start:
+        p.warm_start = args.warm_start
+        cfg = dict(cfg, warm_start={2: "inertial", 3: "learned (colb_b200/data/warmstart_net16.npz)"}[args.warm_start])
     eng = Engine(p, scenes, device=dev)
+    if args.warm_start == 3:
+        from colb_b200 import learned as Lr
+        params, norm, _ = Lr.load()
+        eng.set_mlp(params, norm)
     nb = dynamic_bodies(scenes)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
@@ -204,6 +236,9 @@ def run_ours(args, rank, world):
         dist.barrier()
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
+    if args.profile:
+        return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
+                    lin=lin, e2e_s=float("nan"), clocks=clk.summary(), phases=None, n_timing=0, bytes_state=48 * 8 * eng.nb)
     # ---- e2e through the public API with host buffers: H2D of the state,
     # one step, D2H of the state every step
     host_state = eng.get_state()
@@ -278,7 +313,10 @@ def main():
     ap.add_argument("--workload", default="net16", choices=["net16", "net16c", "chain", "cubes", "batch"])
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed FP32/FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--warm-start", type=int, default=0, choices=[0, 2, 3], help="0 plain, 2 inertial, 3 learned network")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed / learned / batched measurements")
+    ap.add_argument("--profile", action="store_true",
+                    help="timed steps only (no end-to-end, phase-timer, forms or CPU passes): the command to run under ncu")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -304,6 +342,13 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     r = run_ours(args, rank, world)
     nb_total = r["nb"] * world
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": nb_total * args.steps / (r["max_ms"] / 1000.0),
+                              "unit": "body-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                              "profile_run": True, "gpu_launches": r["launches"],
+                              "newton_iters_per_step": r["iters"] / (args.steps * len(r["scenes"]))}))
+        return
     value = nb_total * args.steps / (r["max_ms"] / 1000.0)
     e2e = nb_total * args.steps / r["e2e_s"]
     peak, peak_kind = measured_peaks()

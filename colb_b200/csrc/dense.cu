@@ -318,7 +318,7 @@ static int dense_reserve(Engine* E, DenseState* D, size_t a_elems, size_t rhs_el
     size_t es = sizeof(T);
     if (a_elems * es > D->A_bytes) {
         if (D->A) cudaFree(D->A);
-        D->A_bytes = a_elems * es + (a_elems * es) / 4;
+        D->A_bytes = std::max(a_elems * es * 2, (size_t)1 << 20);
         if (cudaMalloc(&D->A, D->A_bytes) != cudaSuccess) { D->A = nullptr; D->A_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc dense matrices"); }
     }
     if (rhs_elems * es > D->rhs_bytes) {
@@ -327,6 +327,8 @@ static int dense_reserve(Engine* E, DenseState* D, size_t a_elems, size_t rhs_el
         if (cudaMalloc(&D->rhs, D->rhs_bytes) != cudaSuccess) { D->rhs = nullptr; D->rhs_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc dense rhs"); }
     }
     if (nmax > D->work_n || D->work_bytes % es) {
+        // room for components up to twice this size (at most the whole handle)
+        nmax = std::min(std::max(2 * nmax, 384), std::max(12 * E->nb, nmax));
         if (D->work) cudaFree(D->work);
         if (D->ipiv) cudaFree(D->ipiv);
         D->work = nullptr; D->ipiv = nullptr;
@@ -431,6 +433,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         else D->bmap[b] = D->root[r];
     }
     const int nsmall = (int)small_root.size(), nlarge = (int)large_n.size();
+
     if (aoff * (long long)sizeof(T) > (4LL << 30)) { *fallback = 1; return ABD_OK; }
     // local body index inside its component (body order) and the small
     // components' body lists, packed into one upload

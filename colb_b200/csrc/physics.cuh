@@ -332,48 +332,6 @@ DV double d2_pt_plane_full(d3 p, d3 t0, d3 t1, d3 t2, double* g, double* H) {
     return f;
 }
 
-// ---------------------------------------------------------- PSD project
-// H (n x n, row-major, symmetric) <- V max(L, 0) V^T by cyclic Jacobi.
-DV void psd_project(int n, double* H) {
-    double A[144], V[144];
-    double fro = 0;
-    for (int i = 0; i < n * n; i++) { A[i] = H[i]; fro += H[i] * H[i]; }
-    if (fro == 0.0) return;
-    for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) V[i*n+j] = (i == j) ? 1.0 : 0.0;
-    // a rotation is skipped when |a_pq| is at rounding level against the
-    // diagonal; the sweeps stop when none was applied (scale-invariant)
-    for (int sweep = 0; sweep < 50; sweep++) {
-        int rotated = 0;
-        for (int p = 0; p < n; p++)
-            for (int q = p + 1; q < n; q++) {
-                double apq = A[p*n+q];
-                if (fabs(apq) <= fmax(1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])), 1e-16 * sqrt(fro))) continue;
-                rotated = 1;
-                double theta = (A[q*n+q] - A[p*n+p]) / (2 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-                double c = rsqrt(t * t + 1), s = t * c;
-                for (int k = 0; k < n; k++) {
-                    double akp = A[k*n+p], akq = A[k*n+q];
-                    A[k*n+p] = c * akp - s * akq; A[k*n+q] = s * akp + c * akq;
-                }
-                for (int k = 0; k < n; k++) {
-                    double apk = A[p*n+k], aqk = A[q*n+k];
-                    A[p*n+k] = c * apk - s * aqk; A[q*n+k] = s * apk + c * aqk;
-                }
-                for (int k = 0; k < n; k++) {
-                    double vkp = V[k*n+p], vkq = V[k*n+q];
-                    V[k*n+p] = c * vkp - s * vkq; V[k*n+q] = s * vkp + c * vkq;
-                }
-            }
-        if (!rotated) break;
-    }
-    for (int i = 0; i < n; i++)
-        for (int j = 0; j < n; j++) {
-            double s = 0;
-            for (int k = 0; k < n; k++) { double l = A[k*n+k]; if (l > 0) s += V[i*n+k] * l * V[j*n+k]; }
-            H[i*n+j] = s;
-        }
-}
 
 // ------------------------------------------------------------ additive CCD
 // kind 0: edge-edge (x0 x1 | x2 x3), kind 1: point-triangle (x0 | x1 x2 x3).

@@ -9,7 +9,9 @@
 // sweep.  A rotation is skipped when |a_pq| is at rounding level against its
 // diagonal pair or against the whole matrix (rank-deficient Hessians drive
 // some diagonals to zero); sweeps stop when none was applied, the same
-// criterion the serial oracle uses.  A matrix whose Cholesky factorization
+// criterion the serial oracle uses.  The entry a rotation annihilates is set
+// to zero (not left at rounding level), so the sweeps end once the
+// off-diagonal mass has decayed.  A matrix whose Cholesky factorization
 // succeeds is left as it is (it is its own projection).
 #pragma once
 #include "common.cuh"
@@ -108,6 +110,8 @@ DV void warp_psd_project(WarpEigSmem& S, int n) {
                 if (pj >= 0) v += ci * sj * S.A[i*12+pj];
                 if (pi >= 0) v += si * cj * S.A[pi*12+j];
                 if (pi >= 0 && pj >= 0) v += si * sj * S.A[pi*12+pj];
+                // the entry of a rotated pair is annihilated
+                if (pj == i && S.s[S.pair_of[i]] != 0.0) v = 0.0;
                 S.T[i*12+j] = v;
             }
             __syncwarp();

@@ -328,7 +328,9 @@ double oracle_pt_dist2(const double p[3], const double a[3], const double b[3], 
 /* Symmetric eigen-decomposition by cyclic Jacobi rotations and the PSD  */
 /* projection V max(L,0) V^T (used where the reference calls            */
 /* x_to_grad_psd_hess_ee, abd.py:247).  A matrix whose Cholesky         */
-/* factorization succeeds is returned unchanged.                         */
+/* factorization succeeds is returned unchanged.  The entry a rotation  */
+/* annihilates is set to zero rather than left at rounding level, so   */
+/* the sweeps end once the off-diagonal mass has decayed.                */
 /* ------------------------------------------------------------------ */
 /* Cholesky without storing the factor: 1 when every pivot is positive, in
  * which case the matrix is its own PSD projection. */
@@ -377,6 +379,7 @@ void oracle_psd_project(int n, double* H) {
                 double vkp = V[k*n+p], vkq = V[k*n+q];
                 V[k*n+p] = c*vkp - s*vkq; V[k*n+q] = s*vkp + c*vkq;
             }
+            A[p*n+q] = A[q*n+p] = 0.0;      /* the rotation annihilates it */
         }
         if (!rotated) break;
     }
