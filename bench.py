@@ -37,7 +37,7 @@ import numpy as np  # noqa: E402
 METRIC = "ABD body-steps/s @1e-5 residual: learned+batched vs plain, same B200; iters/step"
 
 
-def make_workload(name, rank=0, precision=0, ns_batch=512):
+def make_workload(name, rank=0, precision=0, ns_batch=512, world=1):
     from colb_b200 import params as P, scene as S
     if name == "net16":
         from colb_b200 import fixtures
@@ -67,11 +67,15 @@ def make_workload(name, rank=0, precision=0, ns_batch=512):
         cfg = dict(workload="cubes: 8 unit cubes 2x2x2, ground plane, dt 1/120", bodies=8)
         return [sc], p, cfg
     if name == "batch":
-        scenes = S.config3_batch(n_scenes=ns_batch, seed=rank)
+        # ns_batch scenes per GPU: world * ns_batch seeded scenes partitioned
+        # across ranks by primitive count (colb_b200/shard.py)
+        from colb_b200 import shard
+        allsc = S.config3_batch(n_scenes=ns_batch * world, seed=0)
+        scenes, _ = shard.shard(allsc, rank, world)
         p = P.config_params(precision=precision)
         nb = sum(len(s["mass"]) for s in scenes)
-        cfg = dict(workload=f"batch: {ns_batch} scenes of 4..64 cubes/tori (log-uniform), ground, dt 1/120",
-                   bodies=nb, scenes=ns_batch)
+        cfg = dict(workload=f"batch: {ns_batch} scenes per GPU of 4..64 cubes/tori (log-uniform), ground, dt 1/120",
+                   bodies=nb, scenes=len(scenes), scenes_total=len(allsc))
         return scenes, p, cfg
     raise SystemExit(f"unknown workload {name}")
 
@@ -200,7 +204,7 @@ def run_ours(args, rank, world):
     from colb_b200.engine import Engine
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    scenes, p, cfg = make_workload(args.workload, rank, args.precision)
+    scenes, p, cfg = make_workload(args.workload, rank, args.precision, world=world)
     if args.warm_start:
         p.warm_start = args.warm_start
         cfg = dict(cfg, warm_start={2: "inertial", 3: "learned (colb_b200/data/warmstart_net16.npz)"}[args.warm_start])
@@ -236,6 +240,12 @@ def run_ours(args, rank, world):
         dist.barrier()
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
+    # bodies over all ranks (scene shards differ in size)
+    nbt = torch.tensor([float(nb)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(nbt)
+    nb = int(nbt.item()) if world > 1 else nb
     if args.profile:
         return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
                     lin=lin, e2e_s=float("nan"), clocks=clk.summary(), phases=None, n_timing=0, bytes_state=48 * 8 * eng.nb)
@@ -341,7 +351,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     r = run_ours(args, rank, world)
-    nb_total = r["nb"] * world
+    nb_total = r["nb"]
     if args.profile:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": nb_total * args.steps / (r["max_ms"] / 1000.0),
