@@ -121,12 +121,15 @@ __global__ void __launch_bounds__(32 * BA_WARPS) k_body_assemble(int nb, const d
             double qt = now[ST_Q + r] + dt * now[ST_QD + r];
             g[lane] = dt * dt * (gi * 4.0 * k_ortho) + (q[r] - qt) * Jb;
         }
-        for (int e = lane; e < 81; e += 32) {
-            int rr = e / 9, cc = e % 9;
-            E.A[rr*12 + cc] = ortho_hess(q, k_ortho, rr / 3, cc / 3, rr % 3, cc % 3) * dt * dt;
+        if (project) {
+            ortho_hess_psd_warp(q, k_ortho * dt * dt, E.A, lane);    // analytic eigensystem
+        } else {
+            for (int e = lane; e < 81; e += 32) {
+                int rr = e / 9, cc = e % 9;
+                E.A[rr*12 + cc] = ortho_hess(q, k_ortho, rr / 3, cc / 3, rr % 3, cc % 3) * dt * dt;
+            }
         }
         __syncwarp();
-        if (project) warp_psd_project(E, 9);
         for (int e = lane; e < 144; e += 32) {
             int row = e % 12, col = e / 12;
             double v;
@@ -329,6 +332,25 @@ __global__ void __launch_bounds__(32 * CA_WARPS) k_contact_assemble(const Counte
                 int i = e / m, j = e % m;
                 double h = (C.type == T_PP) ? 0.0 : B1 * A[i*12+j];       // abd.py:381-382
                 A[i*12+j] = (h + B2 * C.g[i] * C.g[j]) * sc;
+            }
+            __syncwarp();
+        } else if (C.type == T_PG || C.type == T_PP) {
+            // analytic projection.  With d the separation (g = 2d on the first
+            // point), B1 H + B2 g g^T is [M] (point-plane, d along the normal)
+            // or [M -M; -M M] (point-point) with M = 2 B1 I + 4 B2 d d^T for
+            // point-point and M = (2 B1 + 4 B2 d^2) n n^T for point-plane; the
+            // projection clamps M's eigenvalues 2 B1 (across d) and
+            // 2 B1 + 4 B2 |d|^2 (along d) at zero.
+            const double dx = 0.5 * C.g[0], dy = 0.5 * C.g[1], dz = 0.5 * C.g[2];
+            const double dd = dx * dx + dy * dy + dz * dz;
+            const double lam_t = C.type == T_PP ? fmax(2.0 * B1, 0.0) : 0.0;
+            const double lam_n = fmax(2.0 * B1 + 4.0 * B2 * dd, 0.0);
+            const double dv[3] = {dx, dy, dz};
+            for (int e = lane; e < m * m; e += 32) {
+                int i = e / m, j = e % m, a = i % 3, b = j % 3;
+                double nn = dd > 0.0 ? dv[a] * dv[b] / dd : 0.0;
+                double Mab = lam_t * ((a == b ? 1.0 : 0.0) - nn) + lam_n * nn;
+                A[i*12+j] = ((i / 3) == (j / 3) ? Mab : -Mab) * sc;
             }
             __syncwarp();
         } else {

@@ -89,6 +89,102 @@ DV double ortho_hess(const double* q, double k, int i, int j, int r, int c) {
     return v * 4.0 * k;
 }
 
+// Singular value decomposition A = U diag(s) V^T of a 3x3 matrix (row-major):
+// cyclic Jacobi on A^T A (annihilated entries set to zero), u_i = A v_i / s_i,
+// a vanishing singular value's u completed by a cross product.
+DV void svd3(const double* A, double* U, double* s, double* V) {
+    double S[9];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) S[3*i+j] = A[i] * A[j] + A[3+i] * A[3+j] + A[6+i] * A[6+j];
+    for (int i = 0; i < 9; i++) V[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    const double tr = S[0] + S[4] + S[8];
+    for (int sweep = 0; sweep < 16; sweep++) {
+        double off = S[1] * S[1] + S[2] * S[2] + S[5] * S[5];
+        if (!(off > 1e-34 * tr * tr)) break;
+        for (int pq = 0; pq < 3; pq++) {
+            int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+            double apq = S[3*p+q];
+            if (apq == 0.0) continue;
+            double theta = (S[3*q+q] - S[3*p+p]) / (2 * apq);
+            double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+            double c = 1.0 / sqrt(t * t + 1), sn = t * c;
+            for (int k = 0; k < 3; k++) {          // S <- S R
+                double skp = S[3*k+p], skq = S[3*k+q];
+                S[3*k+p] = c * skp - sn * skq; S[3*k+q] = sn * skp + c * skq;
+            }
+            for (int k = 0; k < 3; k++) {          // S <- R^T S
+                double spk = S[3*p+k], sqk = S[3*q+k];
+                S[3*p+k] = c * spk - sn * sqk; S[3*q+k] = sn * spk + c * sqk;
+            }
+            S[3*p+q] = S[3*q+p] = 0.0;
+            for (int k = 0; k < 3; k++) {          // V <- V R
+                double vkp = V[3*k+p], vkq = V[3*k+q];
+                V[3*k+p] = c * vkp - sn * vkq; V[3*k+q] = sn * vkp + c * vkq;
+            }
+        }
+    }
+    double smax = 0;
+    for (int i = 0; i < 3; i++) { s[i] = sqrt(fmax(S[4*i], 0.0)); smax = fmax(smax, s[i]); }
+    bool ok[3];
+    for (int i = 0; i < 3; i++) {
+        ok[i] = s[i] > 1e-12 * smax && s[i] > 0.0;
+        for (int r = 0; r < 3; r++)
+            U[3*r+i] = ok[i] ? (A[3*r] * V[i] + A[3*r+1] * V[3+i] + A[3*r+2] * V[6+i]) / s[i] : 0.0;
+    }
+    for (int i = 0; i < 3; i++) {
+        if (ok[i]) continue;
+        int j = (i + 1) % 3, k = (i + 2) % 3;
+        d3 uj = mk3(U[j], U[3+j], U[6+j]), uk = mk3(U[k], U[3+k], U[6+k]);
+        d3 w = cross(uj, uk);
+        if (!(dot(w, w) > 0.5)) w = ok[j] ? (fabs(uj.x) < 0.9 ? cross(uj, mk3(1, 0, 0)) : cross(uj, mk3(0, 1, 0)))
+                                          : mk3(i == 0, i == 1, i == 2);
+        double n = sqrt(dot(w, w));
+        U[i] = w.x / n; U[3+i] = w.y / n; U[6+i] = w.z / n;
+        ok[i] = true;
+    }
+}
+
+// PSD projection of the Hessian of k ||A A^T - I||_F^2 (A = q, entries in
+// row-major order) from its analytic eigensystem: the energy is isotropic,
+// psi(s) = sum (s_i^2 - 1)^2 of the singular values of A = U S V^T, and
+// (Smith, de Goes, Kim 2019, "Analytic eigensystems for isotropic distortion
+// energies") its nine eigenpairs are
+//   U e_i e_i^T V^T                       12 s_i^2 - 4
+//   U (e_i e_j^T + e_j e_i^T) V^T / sqrt2   4 (s_i^2 + s_i s_j + s_j^2 - 1)
+//   U (e_i e_j^T - e_j e_i^T) V^T / sqrt2   4 (s_i^2 - s_i s_j + s_j^2 - 1)
+// (times k).  Each lane of a warp writes its entries of out (ld 12) times
+// scale; all 32 lanes call it.
+DV void ortho_hess_psd_warp(const double* q, double scale, double* out, int lane) {
+    double U[9], s[3], V[9];
+    svd3(q, U, s, V);
+    double lam[9], vec[9][9];
+    int m = 0;
+    const double r2 = 0.70710678118654752440;
+    for (int i = 0; i < 3; i++, m++) {
+        lam[m] = 12.0 * s[i] * s[i] - 4.0;
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) vec[m][3*r+c] = U[3*r+i] * V[3*c+i];
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = i + 1; j < 3; j++) {
+            lam[m] = 4.0 * (s[i] * s[i] + s[i] * s[j] + s[j] * s[j] - 1.0);
+            lam[m + 1] = 4.0 * (s[i] * s[i] - s[i] * s[j] + s[j] * s[j] - 1.0);
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) {
+                    double a = U[3*r+i] * V[3*c+j], b = U[3*r+j] * V[3*c+i];
+                    vec[m][3*r+c] = (a + b) * r2;
+                    vec[m + 1][3*r+c] = (a - b) * r2;
+                }
+            m += 2;
+        }
+    for (int e = lane; e < 81; e += 32) {
+        int a = e / 9, b = e % 9;
+        double acc = 0;
+        for (int k = 0; k < 9; k++) if (lam[k] > 0) acc += lam[k] * vec[k][a] * vec[k][b];
+        out[a * 12 + b] = acc * scale;
+    }
+}
+
 // ------------------------------------------------- segment closest points
 // Every float operation is one IEEE round-to-nearest (no contraction), so
 // the result is bit-identical to a C evaluation without FMA contraction.
