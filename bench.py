@@ -295,21 +295,27 @@ def run_forms(args, scenes, p, dev=0):
              "batched_x8": ({}, 8, False), "learned+batched_x8+mixed": (dict(precision=1, warm_start=3), 8, True)}
     out = {}
     for name, (over, copies, learned) in forms.items():
-        e = Engine(params_from_dict(dict(base, **over)), list(scenes) * copies, device=dev)
-        if learned:
-            e.set_mlp(params, norm)
-        nb = dynamic_bodies(scenes) * copies
-        for _ in range(2):
-            e.step(1, allow=(-6, -7))
-        torch.cuda.synchronize()
-        ms = it = unconv = 0
-        for _ in range(steps):
-            rc, st = e.step(1, allow=(-6, -7))
-            ms += st.gpu_ms; it += st.newton_iters; unconv += st.unconverged
-        out[name] = {"value": nb * steps / (ms / 1000.0), "unit": "body-steps/s",
-                     "newton_iters_per_step": it / (steps * len(scenes) * copies), "unconverged_steps": unconv,
-                     "steps": steps, "intersections": e.count_intersections()}
-        e.close()
+        e = None
+        try:
+            e = Engine(params_from_dict(dict(base, **over)), list(scenes) * copies, device=dev)
+            if learned:
+                e.set_mlp(params, norm)
+            nb = dynamic_bodies(scenes) * copies
+            for _ in range(2):
+                e.step(1, allow=(-6, -7))
+            torch.cuda.synchronize()
+            ms = it = unconv = 0
+            for _ in range(steps):
+                rc, st = e.step(1, allow=(-6, -7))
+                ms += st.gpu_ms; it += st.newton_iters; unconv += st.unconverged
+            out[name] = {"value": nb * steps / (ms / 1000.0), "unit": "body-steps/s",
+                         "newton_iters_per_step": it / (steps * len(scenes) * copies), "unconverged_steps": unconv,
+                         "steps": steps, "intersections": e.count_intersections()}
+        except Exception as ex:                      # report the form as failed, keep the line
+            out[name] = {"error": str(ex)}
+        finally:
+            if e is not None:
+                e.close()
     out["learned_model"] = dict(meta, file="colb_b200/data/warmstart_net16.npz")
     return out
 

@@ -90,7 +90,11 @@ class AbdStepStats(C.Structure):
         ("min_toi", C.c_double),
         ("gpu_ms", C.c_double),
         ("kernel_launches", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("comp_band", C.c_int32),
+        ("comp_small", C.c_int32),
+        ("comp_large", C.c_int32),
+        ("krylov_fallbacks", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
     def as_dict(self):

@@ -63,16 +63,6 @@ __global__ void k_block_rows(int nb, const unsigned long long* __restrict__ ukey
     if (blockIdx.x == 0 && threadIdx.x == 0) { row_ptr[nb] = m; cnt->nnzb = m; }
 }
 
-DV int find_block(const int* row_ptr, const int* bcol, int r, int c) {
-    int lo = row_ptr[r], hi = row_ptr[r+1] - 1;
-    while (lo <= hi) {
-        int mid = (lo + hi) >> 1;
-        int v = bcol[mid];
-        if (v == c) return mid;
-        if (v < c) lo = mid + 1; else hi = mid - 1;
-    }
-    return -1;
-}
 
 template <class T>
 __global__ void k_zero_vals(const Counters* cnt, T* vals) {

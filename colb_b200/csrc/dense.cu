@@ -6,10 +6,13 @@
 // edges are the off-diagonal 12x12 blocks (two dynamic bodies joined by an
 // active contact).  A component is factored on its own:
 //   - one body: the 12x12 block inverse written by the assembly;
-//   - up to SMALL_MAX_BODIES bodies: one CTA per component factors it in
-//     shared memory (blocked Cholesky by 12-wide body columns; LU with
-//     partial pivoting when a pivot is not positive), all such components
-//     in one launch;
+//   - Hessian projected to PSD and, in reverse Cuthill-McKee order, a body
+//     bandwidth of at most BAND_MAX: one CTA per component runs a banded
+//     block Cholesky with a sliding window in shared memory, all such
+//     components in one launch;
+//   - otherwise up to SMALL_MAX_BODIES bodies: one CTA per component factors
+//     it in shared memory (blocked Cholesky by 12-wide body columns; LU with
+//     partial pivoting when a pivot is not positive), all in one launch;
 //   - larger components: the 12x12 blocks are scattered into a dense
 //     column-major matrix and factored with cuSOLVER (Cholesky, or LU when
 //     Cholesky reports a non-positive pivot).
@@ -53,7 +56,8 @@ __global__ void k_rhs_gather(int nb, const double* __restrict__ g, const int* __
 }
 // du of every body: large components from their dense solution, single
 // bodies from their 12x12 block inverse (column-major); bodies of small
-// components (bcomp -2) were written by k_small_solve
+// components (bcomp -2) and band components (-3) were written by
+// k_small_solve / k_band_solve
 template <class T>
 __global__ void k_du_scatter(int nb, const double* __restrict__ g, const int* __restrict__ bcomp,
                              const int* __restrict__ blocal, const long long* __restrict__ comp_rhs,
@@ -63,7 +67,7 @@ __global__ void k_du_scatter(int nb, const double* __restrict__ g, const int* __
         int b = (int)(i / 12), r = (int)(i % 12);
         if (ndone[bscene[b]]) continue;
         int c = bcomp[b];
-        if (c == -2) continue;
+        if (c <= -2) continue;
         if (c >= 0) { du[i] = (double)x[comp_rhs[c] + 12L * blocal[b] + r]; continue; }
         const T* D = dinv + 144L * b;
         double acc = 0;
@@ -261,6 +265,165 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_solve(int nsmall, const
     }
 }
 
+
+// ------------------------------------------------------------------ band components
+// A component whose bodies, in reverse Cuthill-McKee order, couple only
+// bodies at most BAND_MAX apart is a block band matrix: its Cholesky factor
+// has the same band.  One CTA factors it with a sliding window of
+// (BAND_MAX + 1)^2 12x12 blocks in shared memory (block column k: factor the
+// diagonal block, solve the panel below, update the window, load the next
+// block row), eliminating the right-hand side on the way (L y = g); the
+// factor's block columns go to global scratch for the backward solve
+// L^T du = y.  No host synchronisation, all band components in one launch.
+constexpr int BAND_MAX = 8;
+constexpr int BAND_W = BAND_MAX + 1;
+constexpr int BAND_THREADS = 256;
+
+template <class T>
+__device__ void band_load_block(T* dst, int bi_body, int bj_body, const int* __restrict__ row_ptr,
+                                const int* __restrict__ bcol, const T* __restrict__ vals, int lane) {
+    int bi = find_block(row_ptr, bcol, bi_body, bj_body);
+    for (int e = lane; e < 144; e += 32) {
+        int r = e / 12, c = e % 12;
+        dst[e] = bi >= 0 ? vals[(long)bi * 144 + c * 12 + r] : (T)0;     // row-major from column-major
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const int* __restrict__ cptr,
+        const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
+        const int* __restrict__ row_ptr, const int* __restrict__ bcol, const T* __restrict__ vals,
+        const double* __restrict__ g, T* Lg, double* du, int* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* win = (T*)smem_raw;                                   // [BAND_W][BAND_W][144], row-major blocks
+    T* rhs = win + BAND_W * BAND_W * 144;                    // [BAND_W][12]
+    T* part = rhs + BAND_W * 12;                             // [BAND_MAX][12]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int cc = blockIdx.x; cc < ncomp; cc += gridDim.x) {
+        const int* ord = order + cptr[cc];
+        const int N = cptr[cc + 1] - cptr[cc], wb = cbw[cc];
+        T* L = Lg + loff[cc] * 144;                          // block (k, d) of L(k + d, k) at (k * BAND_W + d)
+        auto slot = [&](int i, int j) { return win + ((i % BAND_W) * BAND_W + (j % BAND_W)) * 144; };
+        // window rows 0..min(wb, N - 1)
+        const int r0 = min(wb, N - 1);
+        for (int q = warp; q < (r0 + 1) * (r0 + 1); q += nw) {
+            int i = q / (r0 + 1), j = q % (r0 + 1);
+            if (j <= i) band_load_block<T>(slot(i, j), ord[i], ord[j], row_ptr, bcol, vals, lane);
+        }
+        for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) % BAND_W * 12 + e % 12] = (T)g[12L * ord[e / 12] + e % 12];
+        __syncthreads();
+        for (int k = 0; k < N; k++) {
+            const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
+            T* D = slot(k, k);
+            T* yk = rhs + (k % BAND_W) * 12;
+            if (warp == 0) {
+                // D = L_kk L_kk^T (lower, in place), then y_k = L_kk^-1 rhs_k
+                for (int j = 0; j < 12; j++) {
+                    if (lane == 0) {
+                        T d = D[j * 12 + j];
+                        if (!(d > (T)0)) { atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
+                        D[j * 12 + j] = sqrt(d);
+                    }
+                    __syncwarp();
+                    T djj = D[j * 12 + j];
+                    if (lane > j && lane < 12) D[lane * 12 + j] /= djj;
+                    __syncwarp();
+                    if (lane > j && lane < 12) {
+                        T lij = D[lane * 12 + j];
+                        for (int c2 = j + 1; c2 <= lane; c2++) D[lane * 12 + c2] -= lij * D[c2 * 12 + j];
+                    }
+                    __syncwarp();
+                }
+                T v = lane < 12 ? yk[lane] : (T)0;
+                for (int t = 0; t < 12; t++) {
+                    T yt = __shfl_sync(0xffffffffu, v, t) / D[t * 12 + t];
+                    if (lane == t) v = yt;
+                    if (lane > t && lane < 12) v -= D[lane * 12 + t] * yt;
+                }
+                if (lane < 12) { yk[lane] = v; du[12L * ord[k] + lane] = (double)v; }
+            }
+            __syncthreads();
+            // panel: L_ik = A_ik L_kk^-T, one thread per block row
+            for (int t = tid; t < 12 * nk; t += blockDim.x) {
+                int i = k + 1 + t / 12, r = t % 12;
+                T* R = slot(i, k) + r * 12;
+                for (int j = 0; j < 12; j++) {
+                    T a = R[j];
+                    for (int s = 0; s < j; s++) a -= R[s] * D[j * 12 + s];
+                    R[j] = a / D[j * 12 + j];
+                }
+            }
+            __syncthreads();
+            // factor column to global; rhs_i -= L_ik y_k; window update A_ij -= L_ik L_jk^T
+            for (int e = tid; e < (nk + 1) * 144; e += blockDim.x) {
+                int d = e / 144;
+                L[((long)k * BAND_W + d) * 144 + e % 144] = slot(k + d, k)[e % 144];
+            }
+            for (int t = tid; t < 12 * nk; t += blockDim.x) {
+                int i = k + 1 + t / 12, r = t % 12;
+                const T* R = slot(i, k) + r * 12;
+                T acc = 0;
+#pragma unroll
+                for (int c2 = 0; c2 < 12; c2++) acc += R[c2] * yk[c2];
+                rhs[(i % BAND_W) * 12 + r] -= acc;
+            }
+            const int npair = nk * (nk + 1) / 2;
+            for (int e = tid; e < npair * 144; e += blockDim.x) {
+                int p = e / 144, rc = e % 144;
+                int a = 0; while ((a + 1) * (a + 2) / 2 <= p) a++;
+                int b = p - a * (a + 1) / 2;                  // b <= a
+                int i = k + 1 + a, j = k + 1 + b;
+                const T* Li = slot(i, k) + (rc / 12) * 12;
+                const T* Lj = slot(j, k) + (rc % 12) * 12;
+                T acc = 0;
+#pragma unroll
+                for (int s = 0; s < 12; s++) acc += Li[s] * Lj[s];
+                slot(i, j)[rc] -= acc;
+            }
+            __syncthreads();
+            // next block row enters the window
+            const int inew = k + 1 + wb;
+            if (inew < N) {
+                for (int q = warp; q < wb + 1; q += nw) {
+                    int j = k + 1 + q;
+                    band_load_block<T>(slot(inew, j), ord[inew], ord[j], row_ptr, bcol, vals, lane);
+                }
+                if (tid < 12) rhs[(inew % BAND_W) * 12 + tid] = (T)g[12L * ord[inew] + tid];
+            }
+            __syncthreads();
+        }
+        // backward: L^T du = y (y in du)
+        for (int k = N - 1; k >= 0; k--) {
+            const int nk = min(wb, N - 1 - k);
+            for (int t = tid; t < 12 * nk; t += blockDim.x) {
+                int d = 1 + t / 12, r = t % 12;              // block L(k + d, k), column r
+                const T* B = L + ((long)k * BAND_W + d) * 144;
+                const double* xi = du + 12L * ord[k + d];
+                T acc = 0;
+#pragma unroll
+                for (int c2 = 0; c2 < 12; c2++) acc += B[c2 * 12 + r] * (T)xi[c2];
+                part[(d - 1) * 12 + r] = acc;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                const T* Dk = L + (long)k * BAND_W * 144;
+                T v = 0;
+                if (lane < 12) {
+                    v = (T)du[12L * ord[k] + lane];
+                    for (int d = 0; d < nk; d++) v -= part[d * 12 + lane];
+                }
+                for (int t = 11; t >= 0; t--) {
+                    T xt = __shfl_sync(0xffffffffu, v, t) / Dk[t * 12 + t];
+                    if (lane == t) v = xt;
+                    if (lane < t) v -= Dk[t * 12 + lane] * xt;
+                }
+                if (lane < 12) du[12L * ord[k] + lane] = (double)v;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 struct DenseState {
     cusolverDnHandle_t h = nullptr;
     void* A = nullptr; size_t A_bytes = 0;
@@ -269,10 +432,14 @@ struct DenseState {
     int* ipiv = nullptr;
     int* info = nullptr;                             // [0] small-component status, then 2 per large component
     long long* comp_d = nullptr;                     // per large component: offset | rhs offset | n
-    int* imap_d = nullptr; int* imap_h = nullptr;    // bmap | blocal | sptr | sbody, pinned staging
+    int* imap_d = nullptr; int* imap_h = nullptr;    // bmap | blocal | sptr | sbody | band cptr | bw | order
+    long long* loff_d = nullptr; long long* loff_h = nullptr;   // band factor offsets (blocks)
+    void* Lg = nullptr; size_t Lg_bytes = 0;         // band factors
     std::vector<unsigned long long> keys;
     std::vector<int> done, parent, size, root, bmap, fill;
+    std::vector<int> adj_ptr, adj, pos, deg, members, mptr, bfs;
     bool smem_set[2] = {false, false};
+    bool band_smem_set[2] = {false, false};
 };
 static DenseState* ds_of(Engine* E) { return reinterpret_cast<DenseState*>(E->dense_state); }
 
@@ -282,9 +449,10 @@ void eng_dense_free(Engine* E) {
     DenseState* D = ds_of(E);
     if (!D) return;
     if (D->h) cusolverDnDestroy(D->h);
-    void* ps[] = {D->A, D->rhs, D->work, D->ipiv, D->info, D->comp_d, D->imap_d};
+    void* ps[] = {D->A, D->rhs, D->work, D->ipiv, D->info, D->comp_d, D->imap_d, D->loff_d, D->Lg};
     for (void* p : ps) if (p) cudaFree(p);
     if (D->imap_h) cudaFreeHost(D->imap_h);
+    if (D->loff_h) cudaFreeHost(D->loff_h);
     delete D;
     E->dense_state = nullptr;
 }
@@ -305,9 +473,11 @@ static int dense_init(Engine* E) {
     E->dense_state = D;
     if (cusolverDnCreate(&D->h) != CUSOLVER_STATUS_SUCCESS) return E->fail(ABD_ERR_CUDA, "cusolverDnCreate");
     cusolverDnSetStream(D->h, E->stream);
-    size_t ni = 4 * (size_t)E->nb + 8;
+    size_t ni = 8 * (size_t)E->nb + 16;
     if (cudaMalloc(&D->imap_d, sizeof(int) * ni) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc maps");
     if (cudaMallocHost(&D->imap_h, sizeof(int) * ni) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMallocHost maps");
+    if (cudaMalloc(&D->loff_d, sizeof(long long) * (E->nb + 1)) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc band offsets");
+    if (cudaMallocHost(&D->loff_h, sizeof(long long) * (E->nb + 1)) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMallocHost band offsets");
     if (cudaMalloc(&D->info, sizeof(int) * (2 * MAX_LARGE_COMPONENTS + 2)) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc info");
     if (cudaMalloc(&D->comp_d, sizeof(long long) * 3 * MAX_LARGE_COMPONENTS) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc comps");
     return ABD_OK;
@@ -405,23 +575,92 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     }
     D->size.assign(nb, 0);
     for (int b = 0; b < nb; b++) D->size[find(b)]++;
-    // components of scenes still iterating: small ones (one CTA each) and large ones (cuSOLVER)
+    const bool projected = E->P.hess_mode == ABD_HESS_PROJECTED;
+    // body adjacency (off-diagonal blocks, both directions are stored)
+    D->adj_ptr.assign(nb + 1, 0);
+    for (int k = 0; k < nk; k++) {
+        unsigned long long key = D->keys[k];
+        if (key == ~0ull) continue;
+        int r = (int)(key / nb), c = (int)(key % nb);
+        if (r != c) D->adj_ptr[r + 1]++;
+    }
+    for (int b = 0; b < nb; b++) D->adj_ptr[b + 1] += D->adj_ptr[b];
+    D->adj.resize(std::max(D->adj_ptr[nb], 1));
+    {
+        std::vector<int> at(D->adj_ptr.begin(), D->adj_ptr.end() - 1);
+        for (int k = 0; k < nk; k++) {           // keys are sorted: neighbours ascending
+            unsigned long long key = D->keys[k];
+            if (key == ~0ull) continue;
+            int r = (int)(key / nb), c = (int)(key % nb);
+            if (r != c) D->adj[at[r]++] = c;
+        }
+    }
+    // members of every multi-body component of a scene still iterating
+    D->mptr.assign(nb + 1, 0);
+    for (int b = 0; b < nb; b++) { int r = find(b); if (D->size[r] >= 2 && !D->done[E->h_bscene[b]]) D->mptr[r + 1]++; }
+    for (int b = 0; b < nb; b++) D->mptr[b + 1] += D->mptr[b];
+    D->members.resize(std::max(D->mptr[nb], 1));
+    {
+        std::vector<int> at(D->mptr.begin(), D->mptr.end() - 1);
+        for (int b = 0; b < nb; b++) { int r = find(b); if (D->size[r] >= 2 && !D->done[E->h_bscene[b]]) D->members[at[r]++] = b; }
+    }
+    // reverse Cuthill-McKee order of a component (BFS from a minimum-degree
+    // body, neighbours by ascending degree, reversed) and its body bandwidth
+    D->pos.assign(nb, -1);
+    auto rcm = [&](int r, std::vector<int>& out) {
+        const int* m = D->members.data() + D->mptr[r];
+        int n = D->mptr[r + 1] - D->mptr[r];
+        auto degree = [&](int b) { return D->adj_ptr[b + 1] - D->adj_ptr[b]; };
+        int start = m[0];
+        for (int i = 1; i < n; i++) if (degree(m[i]) < degree(start)) start = m[i];
+        out.clear(); out.push_back(start); D->pos[start] = 0;
+        std::vector<int> nb_;
+        for (size_t h = 0; h < out.size(); h++) {
+            int u = out[h];
+            nb_.clear();
+            for (int e = D->adj_ptr[u]; e < D->adj_ptr[u + 1]; e++) if (D->pos[D->adj[e]] < 0) nb_.push_back(D->adj[e]);
+            std::sort(nb_.begin(), nb_.end(), [&](int a, int b) { return degree(a) != degree(b) ? degree(a) < degree(b) : a < b; });
+            for (int v : nb_) if (D->pos[v] < 0) { D->pos[v] = 0; out.push_back(v); }
+        }
+        std::reverse(out.begin(), out.end());
+        for (int i = 0; i < (int)out.size(); i++) D->pos[out[i]] = i;
+        int bw = 0;
+        for (int u : out)
+            for (int e = D->adj_ptr[u]; e < D->adj_ptr[u + 1]; e++) bw = std::max(bw, std::abs(D->pos[u] - D->pos[D->adj[e]]));
+        return bw;
+    };
+    // components of scenes still iterating: band components (one CTA each,
+    // Cholesky), small ones (one CTA each, dense in shared memory) and large
+    // ones (cuSOLVER)
     D->root.assign(nb, -1);
     D->bmap.assign(nb, -1);
-    std::vector<int> small_root, large_n;
+    std::vector<int> small_root, large_n, band_cptr(1, 0), band_bw, band_order, ord;
     std::vector<long long> large_off, large_rhs;
-    long long aoff = 0, roff = 0;
-    int nmax_large = 0, nmax_small = 0, small_bodies = 0;
+    long long aoff = 0, roff = 0, lblocks = 0;
+    int nmax_large = 0, nmax_small = 0, small_bodies = 0, nband = 0;
     for (int b = 0; b < nb; b++) {
         int r = find(b), sz = D->size[r];
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
+        if (D->root[r] == -1 && projected) {
+            int bw = rcm(r, ord);
+            if (bw <= BAND_MAX) {
+                D->root[r] = -10 - nband;                 // marks a band component
+                D->loff_h[nband] = lblocks;
+                lblocks += (long long)sz * BAND_W;
+                band_order.insert(band_order.end(), ord.begin(), ord.end());
+                band_cptr.push_back((int)band_order.size());
+                band_bw.push_back(bw);
+                nband++;
+            }
+        }
+        if (D->root[r] <= -10) { D->bmap[b] = -3; continue; }
         if (D->root[r] < 0) {
             if (sz <= SMALL_MAX_BODIES) {
                 D->root[r] = (int)small_root.size();
                 small_root.push_back(r);
                 nmax_small = std::max(nmax_small, 12 * sz);
             } else {
-                if ((int)large_n.size() >= MAX_LARGE_COMPONENTS) { *fallback = 1; return ABD_OK; }
+                if ((int)large_n.size() >= MAX_LARGE_COMPONENTS) { *fallback = 1; E->krylov_fallbacks++; return ABD_OK; }
                 D->root[r] = (int)large_n.size();
                 int n = 12 * sz;
                 large_n.push_back(n); large_off.push_back(aoff); large_rhs.push_back(roff);
@@ -433,8 +672,9 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         else D->bmap[b] = D->root[r];
     }
     const int nsmall = (int)small_root.size(), nlarge = (int)large_n.size();
+    E->comp_band += nband; E->comp_small += nsmall; E->comp_large += nlarge;
 
-    if (aoff * (long long)sizeof(T) > (4LL << 30)) { *fallback = 1; return ABD_OK; }
+    if (aoff * (long long)sizeof(T) > (4LL << 30)) { *fallback = 1; E->krylov_fallbacks++; return ABD_OK; }
     // local body index inside its component (body order) and the small
     // components' body lists, packed into one upload
     int* h = D->imap_h;
@@ -455,11 +695,38 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
             h_blocal[b] = D->fill[nsmall + m]++;
         }
     }
-    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies;
+    // band components: cptr | bandwidth | bodies in order
+    int* h_bcptr = h_sbody + small_bodies;
+    int* h_bbw = h_bcptr + nband + 1;
+    int* h_bord = h_bbw + nband;
+    for (int c = 0; c <= nband; c++) h_bcptr[c] = band_cptr[c];
+    for (int c = 0; c < nband; c++) h_bbw[c] = band_bw[c];
+    for (size_t i = 0; i < band_order.size(); i++) h_bord[i] = band_order[i];
+    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies + 2 * (size_t)nband + 1 + band_order.size();
     CUDA_TRY(cudaMemcpyAsync(D->imap_d, h, sizeof(int) * nints, cudaMemcpyHostToDevice, st));
     const int* d_bmap = D->imap_d; const int* d_blocal = D->imap_d + nb;
     const int* d_sptr = D->imap_d + 2 * nb; const int* d_sbody = d_sptr + nsmall + 1;
-    const bool projected = E->P.hess_mode == ABD_HESS_PROJECTED;
+    CUDA_TRY(cudaMemsetAsync(D->info, 0, sizeof(int), st));      // status of the band and small kernels
+    if (nband > 0) {
+        const int* d_bcptr = d_sbody + small_bodies;
+        const int* d_bbw = d_bcptr + nband + 1;
+        const int* d_bord = d_bbw + nband;
+        size_t need = (size_t)lblocks * 144 * sizeof(T);
+        if (need > D->Lg_bytes) {
+            if (D->Lg) cudaFree(D->Lg);
+            D->Lg_bytes = std::max(2 * need, (size_t)1 << 20);
+            if (cudaMalloc(&D->Lg, D->Lg_bytes) != cudaSuccess) { D->Lg = nullptr; D->Lg_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc band factors"); }
+        }
+        CUDA_TRY(cudaMemcpyAsync(D->loff_d, D->loff_h, sizeof(long long) * nband, cudaMemcpyHostToDevice, st));
+        const size_t smem = ((size_t)BAND_W * BAND_W * 144 + BAND_W * 12 + BAND_MAX * 12) * sizeof(T);
+        if (!D->band_smem_set[sizeof(T) == 8]) {
+            CUDA_TRY(cudaFuncSetAttribute(k_band_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            D->band_smem_set[sizeof(T) == 8] = true;
+        }
+        k_band_solve<T><<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, E->row_ptr, E->bcol,
+                                                           (const T*)E->vals, E->g, (T*)D->Lg, E->du, D->info);
+        E->launches++;
+    }
     if (nsmall > 0) {
         size_t smem = ((size_t)nmax_small * (nmax_small + 1) + nmax_small) * sizeof(T);
         if (!D->smem_set[sizeof(T) == 8]) {
@@ -468,7 +735,6 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
                                           (int)((nm * (nm + 1) + nm) * sizeof(T))));
             D->smem_set[sizeof(T) == 8] = true;
         }
-        CUDA_TRY(cudaMemsetAsync(D->info, 0, sizeof(int), st));
         k_small_solve<T><<<nsmall, SMALL_THREADS, smem, st>>>(nsmall, d_sptr, d_sbody, d_blocal, E->row_ptr, E->bcol,
                                                               (const T*)E->vals, E->g, projected ? 1 : 0, E->du, D->info);
         E->launches++;

@@ -104,6 +104,7 @@ struct Engine {
     bool mixed = false;
     std::string err;
     int launches = 0;
+    int comp_band = 0, comp_small = 0, comp_large = 0, krylov_fallbacks = 0;   // direct-solver counters
 
     // host-side scene offsets
     std::vector<int> h_body_begin, h_vert_begin, h_edge_begin, h_tri_begin, h_plane_begin;
@@ -213,6 +214,17 @@ inline int grid_for(long n, int block = 256) {
     if (g < 1) g = 1;
     if (g > NUM_SMS * 16) g = NUM_SMS * 16;
     return (int)g;
+}
+// index of block (r, c) in the block CSR, -1 when absent
+DV int find_block(const int* row_ptr, const int* bcol, int r, int c) {
+    int lo = row_ptr[r], hi = row_ptr[r+1] - 1;
+    while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        int v = bcol[mid];
+        if (v == c) return mid;
+        if (v < c) lo = mid + 1; else hi = mid - 1;
+    }
+    return -1;
 }
 #define GS_LOOP(i, n) for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (long)(n); i += (long)gridDim.x * blockDim.x)
 

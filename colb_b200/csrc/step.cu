@@ -132,6 +132,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     E->prof_res.assign(ns, {}); E->prof_alpha.assign(ns, {}); E->prof_iters.assign(ns, {});
     AbdStepStats st; memset(&st, 0, sizeof st); st.min_toi = 1.0;
     int launches0 = E->launches;
+    E->comp_band = E->comp_small = E->comp_large = E->krylov_fallbacks = 0;
     CUDA_TRY(cudaEventRecord(E->ev0, s));
     for (int step = 0; step < n_steps; step++) {
         CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int) * ns, s));
@@ -263,6 +264,8 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     cudaEventElapsedTime(&ms, E->ev0, E->ev1);
     st.gpu_ms = ms;
     st.kernel_launches = E->launches - launches0;
+    st.comp_band = E->comp_band; st.comp_small = E->comp_small; st.comp_large = E->comp_large;
+    st.krylov_fallbacks = E->krylov_fallbacks;
     if (stats) *stats = st;
     if (E->hcnt->ccd_capped) return E->fail(ABD_ERR_CCD_CAP, "CCD iteration cap reached (step clamped conservatively)");
     return ABD_OK;

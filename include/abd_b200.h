@@ -141,7 +141,11 @@ typedef struct AbdStepStats {
     double  min_toi;           /* smallest CCD time of impact seen (1 if none) */
     double  gpu_ms;            /* device time of the call (CUDA events) */
     int32_t kernel_launches;   /* kernels launched by the call */
-    int32_t reserved[5];
+    int32_t comp_band;         /* direct solver: components solved by the band kernel, */
+    int32_t comp_small;        /*   by the shared-memory dense kernel, */
+    int32_t comp_large;        /*   by cuSOLVER (summed over iterations), */
+    int32_t krylov_fallbacks;  /*   and solves handed to the Krylov solver */
+    int32_t reserved[1];
 } AbdStepStats;
 
 typedef struct AbdHandle AbdHandle;
