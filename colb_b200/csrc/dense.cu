@@ -296,21 +296,28 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         const double* __restrict__ g, T* Lg, double* du, int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* win = (T*)smem_raw;                                   // [BAND_W][BAND_W][144], row-major blocks
-    T* rhs = win + BAND_W * BAND_W * 144;                    // [BAND_W][12]
+    T* stage = win + BAND_W * BAND_W * 144;                  // [2][BAND_W][144]: next block row / factor column
+    T* rhs = stage + 2 * BAND_W * 144;                       // [BAND_W][12]
     T* part = rhs + BAND_W * 12;                             // [BAND_MAX][12]
+    T* rdiag = part + BAND_MAX * 12;                         // [12] reciprocals of the diagonal factor
+    __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    if (tid < BAND_MAX * (BAND_MAX + 1) / 2) {
+        int a = 0; while ((a + 1) * (a + 2) / 2 <= tid) a++;
+        tri_a[tid] = (unsigned char)a; tri_b[tid] = (unsigned char)(tid - a * (a + 1) / 2);
+    }
     for (int cc = blockIdx.x; cc < ncomp; cc += gridDim.x) {
         const int* ord = order + cptr[cc];
         const int N = cptr[cc + 1] - cptr[cc], wb = cbw[cc];
-        T* L = Lg + loff[cc] * 144;                          // block (k, d) of L(k + d, k) at (k * BAND_W + d)
+        T* L = Lg + loff[cc] * 144;                          // block L(k + d, k) at (k * BAND_W + d)
         auto slot = [&](int i, int j) { return win + ((i % BAND_W) * BAND_W + (j % BAND_W)) * 144; };
-        // window rows 0..min(wb, N - 1)
+        // window rows 0..min(wb, N - 1) and their right-hand sides
         const int r0 = min(wb, N - 1);
         for (int q = warp; q < (r0 + 1) * (r0 + 1); q += nw) {
             int i = q / (r0 + 1), j = q % (r0 + 1);
             if (j <= i) band_load_block<T>(slot(i, j), ord[i], ord[j], row_ptr, bcol, vals, lane);
         }
-        for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) % BAND_W * 12 + e % 12] = (T)g[12L * ord[e / 12] + e % 12];
+        for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = (T)g[12L * ord[e / 12] + e % 12];
         __syncthreads();
         for (int k = 0; k < N; k++) {
             const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
@@ -322,11 +329,12 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     if (lane == 0) {
                         T d = D[j * 12 + j];
                         if (!(d > (T)0)) { atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
-                        D[j * 12 + j] = sqrt(d);
+                        d = sqrt(d);
+                        D[j * 12 + j] = d;
+                        rdiag[j] = (T)1 / d;
                     }
                     __syncwarp();
-                    T djj = D[j * 12 + j];
-                    if (lane > j && lane < 12) D[lane * 12 + j] /= djj;
+                    if (lane > j && lane < 12) D[lane * 12 + j] *= rdiag[j];
                     __syncwarp();
                     if (lane > j && lane < 12) {
                         T lij = D[lane * 12 + j];
@@ -336,11 +344,25 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 }
                 T v = lane < 12 ? yk[lane] : (T)0;
                 for (int t = 0; t < 12; t++) {
-                    T yt = __shfl_sync(0xffffffffu, v, t) / D[t * 12 + t];
+                    T yt = __shfl_sync(0xffffffffu, v, t) * rdiag[t];
                     if (lane == t) v = yt;
                     if (lane > t && lane < 12) v -= D[lane * 12 + t] * yt;
                 }
                 if (lane < 12) { yk[lane] = v; du[12L * ord[k] + lane] = (double)v; }
+            } else {
+                // meanwhile: block row k + wb (fetched during the previous column)
+                // enters the window, and block row k + 1 + wb is fetched
+                const int t1 = tid - 32, n1 = blockDim.x - 32;
+                if (k >= 1 && k + wb < N) {
+                    const T* src = stage + (k & 1) * BAND_W * 144;
+                    for (int e = t1; e < (wb + 1) * 144; e += n1) slot(k + wb, k + e / 144)[e % 144] = src[e];
+                    if (t1 < 12) rhs[((k + wb) % BAND_W) * 12 + t1] = (T)g[12L * ord[k + wb] + t1];
+                }
+                if (k + 1 + wb < N) {
+                    T* dst = stage + ((k + 1) & 1) * BAND_W * 144;
+                    for (int q = warp - 1; q < wb + 1; q += nw - 1)
+                        band_load_block<T>(dst + q * 144, ord[k + 1 + wb], ord[k + 1 + q], row_ptr, bcol, vals, lane);
+                }
             }
             __syncthreads();
             // panel: L_ik = A_ik L_kk^-T, one thread per block row
@@ -350,7 +372,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 for (int j = 0; j < 12; j++) {
                     T a = R[j];
                     for (int s = 0; s < j; s++) a -= R[s] * D[j * 12 + s];
-                    R[j] = a / D[j * 12 + j];
+                    R[j] = a * rdiag[j];
                 }
             }
             __syncthreads();
@@ -370,9 +392,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             const int npair = nk * (nk + 1) / 2;
             for (int e = tid; e < npair * 144; e += blockDim.x) {
                 int p = e / 144, rc = e % 144;
-                int a = 0; while ((a + 1) * (a + 2) / 2 <= p) a++;
-                int b = p - a * (a + 1) / 2;                  // b <= a
-                int i = k + 1 + a, j = k + 1 + b;
+                int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
                 const T* Li = slot(i, k) + (rc / 12) * 12;
                 const T* Lj = slot(j, k) + (rc % 12) * 12;
                 T acc = 0;
@@ -381,41 +401,43 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 slot(i, j)[rc] -= acc;
             }
             __syncthreads();
-            // next block row enters the window
-            const int inew = k + 1 + wb;
-            if (inew < N) {
-                for (int q = warp; q < wb + 1; q += nw) {
-                    int j = k + 1 + q;
-                    band_load_block<T>(slot(inew, j), ord[inew], ord[j], row_ptr, bcol, vals, lane);
-                }
-                if (tid < 12) rhs[(inew % BAND_W) * 12 + tid] = (T)g[12L * ord[inew] + tid];
-            }
-            __syncthreads();
         }
-        // backward: L^T du = y (y in du)
+        // backward: L^T du = y (y in du); the factor column of k is staged in
+        // shared memory while the previous one is solved
+        {
+            const int k0 = N - 1;
+            for (int e = tid; e < 144; e += blockDim.x) stage[(k0 & 1) * BAND_W * 144 + e] = L[(long)k0 * BAND_W * 144 + e];
+        }
+        __syncthreads();
         for (int k = N - 1; k >= 0; k--) {
             const int nk = min(wb, N - 1 - k);
+            const T* col = stage + (k & 1) * BAND_W * 144;
             for (int t = tid; t < 12 * nk; t += blockDim.x) {
                 int d = 1 + t / 12, r = t % 12;              // block L(k + d, k), column r
-                const T* B = L + ((long)k * BAND_W + d) * 144;
+                const T* B = col + d * 144;
                 const double* xi = du + 12L * ord[k + d];
                 T acc = 0;
 #pragma unroll
                 for (int c2 = 0; c2 < 12; c2++) acc += B[c2 * 12 + r] * (T)xi[c2];
                 part[(d - 1) * 12 + r] = acc;
             }
+            if (k > 0 && tid >= 128) {                        // stage column k - 1
+                const int nk1 = min(wb, N - k);
+                T* dst = stage + ((k - 1) & 1) * BAND_W * 144;
+                for (int e = tid - 128; e < (nk1 + 1) * 144; e += blockDim.x - 128)
+                    dst[e] = L[(long)(k - 1) * BAND_W * 144 + e];
+            }
             __syncthreads();
             if (warp == 0) {
-                const T* Dk = L + (long)k * BAND_W * 144;
                 T v = 0;
                 if (lane < 12) {
                     v = (T)du[12L * ord[k] + lane];
                     for (int d = 0; d < nk; d++) v -= part[d * 12 + lane];
                 }
                 for (int t = 11; t >= 0; t--) {
-                    T xt = __shfl_sync(0xffffffffu, v, t) / Dk[t * 12 + t];
+                    T xt = __shfl_sync(0xffffffffu, v, t) / col[t * 12 + t];
                     if (lane == t) v = xt;
-                    if (lane < t) v -= Dk[t * 12 + lane] * xt;
+                    if (lane < t) v -= col[t * 12 + lane] * xt;
                 }
                 if (lane < 12) du[12L * ord[k] + lane] = (double)v;
             }
@@ -718,7 +740,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
             if (cudaMalloc(&D->Lg, D->Lg_bytes) != cudaSuccess) { D->Lg = nullptr; D->Lg_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc band factors"); }
         }
         CUDA_TRY(cudaMemcpyAsync(D->loff_d, D->loff_h, sizeof(long long) * nband, cudaMemcpyHostToDevice, st));
-        const size_t smem = ((size_t)BAND_W * BAND_W * 144 + BAND_W * 12 + BAND_MAX * 12) * sizeof(T);
+        const size_t smem = ((size_t)BAND_W * BAND_W * 144 + 2 * BAND_W * 144 + BAND_W * 12 + BAND_MAX * 12 + 12) * sizeof(T);
         if (!D->band_smem_set[sizeof(T) == 8]) {
             CUDA_TRY(cudaFuncSetAttribute(k_band_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             D->band_smem_set[sizeof(T) == 8] = true;
