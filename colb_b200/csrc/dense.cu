@@ -6,8 +6,8 @@
 // edges are the off-diagonal 12x12 blocks (two dynamic bodies joined by an
 // active contact).  A component is factored on its own:
 //   - one body: the 12x12 block inverse written by the assembly;
-//   - Hessian projected to PSD and, in reverse Cuthill-McKee order, a body
-//     bandwidth of at most BAND_MAX: one CTA per component runs a banded
+//   - FP64, Hessian projected to PSD and, in reverse Cuthill-McKee order, a
+//     body bandwidth of at most BAND_MAX: one CTA per component runs a banded
 //     block Cholesky with a sliding window in shared memory, all such
 //     components in one launch;
 //   - otherwise up to SMALL_MAX_BODIES bodies: one CTA per component factors
@@ -279,43 +279,78 @@ constexpr int BAND_MAX = 8;
 constexpr int BAND_W = BAND_MAX + 1;
 constexpr int BAND_THREADS = 256;
 
+constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
+constexpr int BAND_PREFER_MAX = 24;    // above this many bodies cuSOLVER is preferred while it has room
+
+// 1/sqrt(d): a single-precision estimate refined by two Newton-Raphson steps
+// r <- r (3 - d r^2) / 2 (each squares the relative error: 2^-23 -> 2^-46 ->
+// below double rounding); outside the single-precision range the
+// double-precision rsqrt is used.
+DV double rsqrt_nr(double d) {
+    if (!(d > 1e-30 && d < 1e30)) return rsqrt(d);
+    double r = (double)rsqrtf((float)d);
+    double h = 0.5 * d;
+    r = r * (1.5 - h * r * r);
+    r = r * (1.5 - h * r * r);
+    return r;
+}
+DV float rsqrt_nr(float d) { return rsqrtf(d); }
+
+// Band blocks of every band component, contiguous: A(i, i - d) of position
+// i (component order), d = 0..BAND_MAX, row-major, at (loff + i BAND_W + d);
+// blocks outside the band or absent are zero.  One warp per block.
 template <class T>
-__device__ void band_load_block(T* dst, int bi_body, int bj_body, const int* __restrict__ row_ptr,
-                                const int* __restrict__ bcol, const T* __restrict__ vals, int lane) {
-    int bi = find_block(row_ptr, bcol, bi_body, bj_body);
-    for (int e = lane; e < 144; e += 32) {
-        int r = e / 12, c = e % 12;
-        dst[e] = bi >= 0 ? vals[(long)bi * 144 + c * 12 + r] : (T)0;     // row-major from column-major
+__global__ void k_band_gather(int npos, const int* __restrict__ pcomp, const int* __restrict__ cptr,
+                              const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
+                              const int* __restrict__ row_ptr, const int* __restrict__ bcol, const T* __restrict__ vals,
+                              T* Ab) {
+    const int lane = threadIdx.x & 31;
+    for (long item = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < (long)npos * BAND_W;
+         item += ((long)gridDim.x * blockDim.x) >> 5) {
+        int p = (int)(item / BAND_W), d = (int)(item % BAND_W);
+        int c = pcomp[p], i = p - cptr[c], j = i - d;
+        int bi = -1;
+        if (j >= 0 && d <= cbw[c]) bi = find_block(row_ptr, bcol, order[p], order[cptr[c] + j]);
+        T* dst = Ab + (loff[c] + (long)i * BAND_W + d) * 144;
+        for (int e = lane; e < 144; e += 32) {
+            int r = e / 12, cc = e % 12;
+            dst[e] = bi >= 0 ? vals[(long)bi * 144 + cc * 12 + r] : (T)0;     // row-major from column-major
+        }
     }
 }
 
 template <class T>
 __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const int* __restrict__ cptr,
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
-        const int* __restrict__ row_ptr, const int* __restrict__ bcol, const T* __restrict__ vals,
-        const double* __restrict__ g, T* Lg, double* du, int* status) {
+        const T* __restrict__ Ab, long long ltot, const double* __restrict__ g, T* Lg, double* du, int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* win = (T*)smem_raw;                                   // [BAND_W][BAND_W][144], row-major blocks
     T* stage = win + BAND_W * BAND_W * 144;                  // [2][BAND_W][144]: next block row / factor column
     T* rhs = stage + 2 * BAND_W * 144;                       // [BAND_W][12]
     T* part = rhs + BAND_W * 12;                             // [BAND_MAX][12]
     T* rdiag = part + BAND_MAX * 12;                         // [12] reciprocals of the diagonal factor
+    T* xs = rdiag + 12;                                      // [BAND_W][12] latest solution blocks (backward)
+    T* srec = xs + BAND_W * 12;                              // [2][12] staged reciprocals (backward)
     __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
+    __shared__ int ord[BAND_ORD_MAX];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
     if (tid < BAND_MAX * (BAND_MAX + 1) / 2) {
         int a = 0; while ((a + 1) * (a + 2) / 2 <= tid) a++;
         tri_a[tid] = (unsigned char)a; tri_b[tid] = (unsigned char)(tid - a * (a + 1) / 2);
     }
     for (int cc = blockIdx.x; cc < ncomp; cc += gridDim.x) {
-        const int* ord = order + cptr[cc];
         const int N = cptr[cc + 1] - cptr[cc], wb = cbw[cc];
+        for (int e = tid; e < N; e += blockDim.x) ord[e] = order[cptr[cc] + e];
         T* L = Lg + loff[cc] * 144;                          // block L(k + d, k) at (k * BAND_W + d)
+        T* Rg = Lg + ltot * 144 + (loff[cc] / BAND_W) * 12; // reciprocal diagonal of L(k, k) at k * 12
+        const T* A = Ab + loff[cc] * 144;                    // block A(i, i - d) at (i * BAND_W + d)
+        __syncthreads();
         auto slot = [&](int i, int j) { return win + ((i % BAND_W) * BAND_W + (j % BAND_W)) * 144; };
         // window rows 0..min(wb, N - 1) and their right-hand sides
         const int r0 = min(wb, N - 1);
-        for (int q = warp; q < (r0 + 1) * (r0 + 1); q += nw) {
-            int i = q / (r0 + 1), j = q % (r0 + 1);
-            if (j <= i) band_load_block<T>(slot(i, j), ord[i], ord[j], row_ptr, bcol, vals, lane);
+        for (int e = tid; e < (r0 + 1) * BAND_W * 144; e += blockDim.x) {
+            int i = e / (BAND_W * 144), d = (e / 144) % BAND_W;
+            if (d <= i) slot(i, i - d)[e % 144] = A[(long)e];
         }
         for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = (T)g[12L * ord[e / 12] + e % 12];
         __syncthreads();
@@ -324,29 +359,41 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             T* D = slot(k, k);
             T* yk = rhs + (k % BAND_W) * 12;
             if (warp == 0) {
-                // D = L_kk L_kk^T (lower, in place), then y_k = L_kk^-1 rhs_k
+                // D = L_kk L_kk^T in registers: lane r < 12 holds row r; the
+                // pivot and its reciprocal square root are computed by every
+                // lane from a broadcast, so the 12 columns need no barrier
+                T a[12];
+#pragma unroll
+                for (int c2 = 0; c2 < 12; c2++) a[c2] = lane < 12 ? D[lane * 12 + c2] : (T)0;
+                T rs[12];
+#pragma unroll
                 for (int j = 0; j < 12; j++) {
-                    if (lane == 0) {
-                        T d = D[j * 12 + j];
-                        if (!(d > (T)0)) { atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
-                        d = sqrt(d);
-                        D[j * 12 + j] = d;
-                        rdiag[j] = (T)1 / d;
+                    T d = __shfl_sync(0xffffffffu, a[j], j);
+                    if (!(d > (T)0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
+                    T r = rsqrt_nr(d);
+                    rs[j] = r;
+                    T l = a[j] * r;                          // L[lane][j] for lane > j
+                    if (lane == j) a[j] = d * r;
+                    if (lane > j) a[j] = l;
+#pragma unroll
+                    for (int c2 = j + 1; c2 < 12; c2++) {
+                        T lc = __shfl_sync(0xffffffffu, l, c2);   // L[c2][j]
+                        if (lane > j) a[c2] -= l * lc;
                     }
-                    __syncwarp();
-                    if (lane > j && lane < 12) D[lane * 12 + j] *= rdiag[j];
-                    __syncwarp();
-                    if (lane > j && lane < 12) {
-                        T lij = D[lane * 12 + j];
-                        for (int c2 = j + 1; c2 <= lane; c2++) D[lane * 12 + c2] -= lij * D[c2 * 12 + j];
-                    }
-                    __syncwarp();
                 }
+                if (lane < 12) {
+#pragma unroll
+                    for (int c2 = 0; c2 < 12; c2++) D[lane * 12 + c2] = c2 <= lane ? a[c2] : (T)0;
+                }
+#pragma unroll
+                for (int j = 0; j < 12; j++) if (lane == j) { rdiag[j] = rs[j]; Rg[(long)k * 12 + j] = rs[j]; }
+                // y_k = L_kk^-1 rhs_k
                 T v = lane < 12 ? yk[lane] : (T)0;
+#pragma unroll
                 for (int t = 0; t < 12; t++) {
-                    T yt = __shfl_sync(0xffffffffu, v, t) * rdiag[t];
+                    T yt = __shfl_sync(0xffffffffu, v, t) * rs[t];
                     if (lane == t) v = yt;
-                    if (lane > t && lane < 12) v -= D[lane * 12 + t] * yt;
+                    if (lane > t && lane < 12) v -= a[t] * yt;
                 }
                 if (lane < 12) { yk[lane] = v; du[12L * ord[k] + lane] = (double)v; }
             } else {
@@ -359,9 +406,10 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     if (t1 < 12) rhs[((k + wb) % BAND_W) * 12 + t1] = (T)g[12L * ord[k + wb] + t1];
                 }
                 if (k + 1 + wb < N) {
+                    // row k + 1 + wb: block j = k + 1 + q is A(., . - d) with d = wb - q
                     T* dst = stage + ((k + 1) & 1) * BAND_W * 144;
-                    for (int q = warp - 1; q < wb + 1; q += nw - 1)
-                        band_load_block<T>(dst + q * 144, ord[k + 1 + wb], ord[k + 1 + q], row_ptr, bcol, vals, lane);
+                    const T* src = A + (long)(k + 1 + wb) * BAND_W * 144;
+                    for (int e = t1; e < (wb + 1) * 144; e += n1) dst[(wb - e / 144) * 144 + e % 144] = src[e];
                 }
             }
             __syncthreads();
@@ -369,11 +417,18 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             for (int t = tid; t < 12 * nk; t += blockDim.x) {
                 int i = k + 1 + t / 12, r = t % 12;
                 T* R = slot(i, k) + r * 12;
+                T x[12];
+#pragma unroll
+                for (int j = 0; j < 12; j++) x[j] = R[j];
+#pragma unroll
                 for (int j = 0; j < 12; j++) {
-                    T a = R[j];
-                    for (int s = 0; s < j; s++) a -= R[s] * D[j * 12 + s];
-                    R[j] = a * rdiag[j];
+                    T a = x[j];
+#pragma unroll
+                    for (int s = 0; s < j; s++) a -= x[s] * D[j * 12 + s];
+                    x[j] = a * rdiag[j];
                 }
+#pragma unroll
+                for (int j = 0; j < 12; j++) R[j] = x[j];
             }
             __syncthreads();
             // factor column to global; rhs_i -= L_ik y_k; window update A_ij -= L_ik L_jk^T
@@ -389,16 +444,32 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 for (int c2 = 0; c2 < 12; c2++) acc += R[c2] * yk[c2];
                 rhs[(i % BAND_W) * 12 + r] -= acc;
             }
+            // A_ij -= L_ik L_jk^T in 3 x 4 tiles (12 per block pair)
             const int npair = nk * (nk + 1) / 2;
-            for (int e = tid; e < npair * 144; e += blockDim.x) {
-                int p = e / 144, rc = e % 144;
+            for (int e = tid; e < npair * 12; e += blockDim.x) {
+                int p = e / 12, tile = e % 12;
                 int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
-                const T* Li = slot(i, k) + (rc / 12) * 12;
-                const T* Lj = slot(j, k) + (rc % 12) * 12;
-                T acc = 0;
+                int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
+                const T* Li = slot(i, k) + r0t * 12;
+                const T* Lj = slot(j, k) + c0t * 12;
+                T acc[3][4] = {};
 #pragma unroll
-                for (int s = 0; s < 12; s++) acc += Li[s] * Lj[s];
-                slot(i, j)[rc] -= acc;
+                for (int s = 0; s < 12; s++) {
+                    T li[3], lj[4];
+#pragma unroll
+                    for (int a2 = 0; a2 < 3; a2++) li[a2] = Li[a2 * 12 + s];
+#pragma unroll
+                    for (int b2 = 0; b2 < 4; b2++) lj[b2] = Lj[b2 * 12 + s];
+#pragma unroll
+                    for (int a2 = 0; a2 < 3; a2++)
+#pragma unroll
+                        for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
+                }
+                T* Aij = slot(i, j);
+#pragma unroll
+                for (int a2 = 0; a2 < 3; a2++)
+#pragma unroll
+                    for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
             }
             __syncthreads();
         }
@@ -407,6 +478,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         {
             const int k0 = N - 1;
             for (int e = tid; e < 144; e += blockDim.x) stage[(k0 & 1) * BAND_W * 144 + e] = L[(long)k0 * BAND_W * 144 + e];
+            if (tid < 12) srec[(k0 & 1) * 12 + tid] = Rg[(long)k0 * 12 + tid];
         }
         __syncthreads();
         for (int k = N - 1; k >= 0; k--) {
@@ -415,10 +487,10 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             for (int t = tid; t < 12 * nk; t += blockDim.x) {
                 int d = 1 + t / 12, r = t % 12;              // block L(k + d, k), column r
                 const T* B = col + d * 144;
-                const double* xi = du + 12L * ord[k + d];
+                const T* xi = xs + ((k + d) % BAND_W) * 12;
                 T acc = 0;
 #pragma unroll
-                for (int c2 = 0; c2 < 12; c2++) acc += B[c2 * 12 + r] * (T)xi[c2];
+                for (int c2 = 0; c2 < 12; c2++) acc += B[c2 * 12 + r] * xi[c2];
                 part[(d - 1) * 12 + r] = acc;
             }
             if (k > 0 && tid >= 128) {                        // stage column k - 1
@@ -426,6 +498,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 T* dst = stage + ((k - 1) & 1) * BAND_W * 144;
                 for (int e = tid - 128; e < (nk1 + 1) * 144; e += blockDim.x - 128)
                     dst[e] = L[(long)(k - 1) * BAND_W * 144 + e];
+                if (tid - 128 < 12) srec[((k - 1) & 1) * 12 + tid - 128] = Rg[(long)(k - 1) * 12 + tid - 128];
             }
             __syncthreads();
             if (warp == 0) {
@@ -434,12 +507,14 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     v = (T)du[12L * ord[k] + lane];
                     for (int d = 0; d < nk; d++) v -= part[d * 12 + lane];
                 }
+                const T* rl = srec + (k & 1) * 12;
+#pragma unroll
                 for (int t = 11; t >= 0; t--) {
-                    T xt = __shfl_sync(0xffffffffu, v, t) / col[t * 12 + t];
+                    T xt = __shfl_sync(0xffffffffu, v, t) * rl[t];
                     if (lane == t) v = xt;
                     if (lane < t) v -= col[t * 12 + lane] * xt;
                 }
-                if (lane < 12) du[12L * ord[k] + lane] = (double)v;
+                if (lane < 12) { du[12L * ord[k] + lane] = (double)v; xs[(k % BAND_W) * 12 + lane] = v; }
             }
             __syncthreads();
         }
@@ -457,6 +532,7 @@ struct DenseState {
     int* imap_d = nullptr; int* imap_h = nullptr;    // bmap | blocal | sptr | sbody | band cptr | bw | order
     long long* loff_d = nullptr; long long* loff_h = nullptr;   // band factor offsets (blocks)
     void* Lg = nullptr; size_t Lg_bytes = 0;         // band factors
+    void* Ab = nullptr;                              // band blocks gathered in component order (Lg_bytes)
     std::vector<unsigned long long> keys;
     std::vector<int> done, parent, size, root, bmap, fill;
     std::vector<int> adj_ptr, adj, pos, deg, members, mptr, bfs;
@@ -471,7 +547,7 @@ void eng_dense_free(Engine* E) {
     DenseState* D = ds_of(E);
     if (!D) return;
     if (D->h) cusolverDnDestroy(D->h);
-    void* ps[] = {D->A, D->rhs, D->work, D->ipiv, D->info, D->comp_d, D->imap_d, D->loff_d, D->Lg};
+    void* ps[] = {D->A, D->rhs, D->work, D->ipiv, D->info, D->comp_d, D->imap_d, D->loff_d, D->Lg, D->Ab};
     for (void* p : ps) if (p) cudaFree(p);
     if (D->imap_h) cudaFreeHost(D->imap_h);
     if (D->loff_h) cudaFreeHost(D->loff_h);
@@ -663,9 +739,15 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     for (int b = 0; b < nb; b++) {
         int r = find(b), sz = D->size[r];
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
-        if (D->root[r] == -1 && projected) {
+        // FP32 roundings of a stiff projected Hessian can make it indefinite:
+        // the band Cholesky (no pivoting, no fallback) runs in FP64 mode only
+        // a single CTA walks the band sequentially, so cuSOLVER (all SMs) is
+        // faster for a component above BAND_PREFER_MAX bodies while few such
+        // components exist
+        if (D->root[r] == -1 && projected && !E->mixed &&
+            (sz <= BAND_PREFER_MAX || (int)large_n.size() >= MAX_LARGE_COMPONENTS / 2)) {
             int bw = rcm(r, ord);
-            if (bw <= BAND_MAX) {
+            if (bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
                 D->root[r] = -10 - nband;                 // marks a band component
                 D->loff_h[nband] = lblocks;
                 lblocks += (long long)sz * BAND_W;
@@ -724,7 +806,10 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     for (int c = 0; c <= nband; c++) h_bcptr[c] = band_cptr[c];
     for (int c = 0; c < nband; c++) h_bbw[c] = band_bw[c];
     for (size_t i = 0; i < band_order.size(); i++) h_bord[i] = band_order[i];
-    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies + 2 * (size_t)nband + 1 + band_order.size();
+    int* h_pcomp = h_bord + band_order.size();
+    for (int c = 0; c < nband; c++)
+        for (int q = band_cptr[c]; q < band_cptr[c + 1]; q++) h_pcomp[q] = c;
+    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies + 2 * (size_t)nband + 1 + 2 * band_order.size();
     CUDA_TRY(cudaMemcpyAsync(D->imap_d, h, sizeof(int) * nints, cudaMemcpyHostToDevice, st));
     const int* d_bmap = D->imap_d; const int* d_blocal = D->imap_d + nb;
     const int* d_sptr = D->imap_d + 2 * nb; const int* d_sbody = d_sptr + nsmall + 1;
@@ -733,20 +818,38 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         const int* d_bcptr = d_sbody + small_bodies;
         const int* d_bbw = d_bcptr + nband + 1;
         const int* d_bord = d_bbw + nband;
-        size_t need = (size_t)lblocks * 144 * sizeof(T);
+        size_t need = ((size_t)lblocks * 144 + 12 * band_order.size()) * sizeof(T);
         if (need > D->Lg_bytes) {
             if (D->Lg) cudaFree(D->Lg);
+            if (D->Ab) cudaFree(D->Ab);
+            D->Ab = nullptr;
             D->Lg_bytes = std::max(2 * need, (size_t)1 << 20);
-            if (cudaMalloc(&D->Lg, D->Lg_bytes) != cudaSuccess) { D->Lg = nullptr; D->Lg_bytes = 0; return E->fail(ABD_ERR_CUDA, "cudaMalloc band factors"); }
+            if (cudaMalloc(&D->Lg, D->Lg_bytes) != cudaSuccess || cudaMalloc(&D->Ab, D->Lg_bytes) != cudaSuccess) {
+                D->Lg_bytes = 0;
+                return E->fail(ABD_ERR_CUDA, "cudaMalloc band factors");
+            }
         }
         CUDA_TRY(cudaMemcpyAsync(D->loff_d, D->loff_h, sizeof(long long) * nband, cudaMemcpyHostToDevice, st));
-        const size_t smem = ((size_t)BAND_W * BAND_W * 144 + 2 * BAND_W * 144 + BAND_W * 12 + BAND_MAX * 12 + 12) * sizeof(T);
+        const size_t smem = ((size_t)BAND_W * BAND_W * 144 + 2 * BAND_W * 144 + BAND_W * 12 + BAND_MAX * 12 + 12 +
+                             BAND_W * 12 + 24) * sizeof(T);
         if (!D->band_smem_set[sizeof(T) == 8]) {
             CUDA_TRY(cudaFuncSetAttribute(k_band_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             D->band_smem_set[sizeof(T) == 8] = true;
         }
-        k_band_solve<T><<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, E->row_ptr, E->bcol,
-                                                           (const T*)E->vals, E->g, (T*)D->Lg, E->du, D->info);
+        const int* d_pcomp = d_bord + band_order.size();
+        const int npos = (int)band_order.size();
+        k_band_gather<T><<<grid_for(32L * npos * BAND_W), 256, 0, st>>>(npos, d_pcomp, d_bcptr, d_bord, d_bbw, D->loff_d,
+                                                                       E->row_ptr, E->bcol, (const T*)E->vals, (T*)D->Ab);
+        E->launches++;
+        int ph = phase_begin(E, PH_BAND);
+        k_band_solve<T><<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, (const T*)D->Ab,
+                                                           lblocks, E->g, (T*)D->Lg, E->du, D->info);
+        // per component: band blocks read, factor written and read back,
+        // g read, y and du written and read
+        double bytes = 0;
+        for (int c = 0; c < nband; c++)
+            bytes += (band_cptr[c + 1] - band_cptr[c]) * ((band_bw[c] + 1) * 144.0 * sizeof(T) * 3 + 96.0 * 4);
+        phase_end(E, ph, bytes);
         E->launches++;
     }
     if (nsmall > 0) {

@@ -187,7 +187,7 @@ struct Engine {
 };
 
 enum { PH_DETECT = 0, PH_ASSEMBLE, PH_SOLVE, PH_ENERGY, PH_CCD, PH_OTHER, PH_EQUERY, PH_SPMV,
-       PH_ASM_KEYS, PH_ASM_BODY, PH_ASM_CONTACT, PH_ASM_INV, PH_DENSE, PH_SWEPT, PH_ELIST, PH_TRIALS };
+       PH_ASM_KEYS, PH_ASM_BODY, PH_ASM_CONTACT, PH_ASM_INV, PH_DENSE, PH_SWEPT, PH_ELIST, PH_TRIALS, PH_BAND };
 
 // Bracket device work with events when timing is on.  phase_begin returns a
 // record index (or -1), phase_end closes it with the algorithmic bytes moved.

@@ -26,7 +26,7 @@ EXPORTS = [
 ]
 MLP_IN, MLP_OUT, MLP_NPARAM, MLP_NNORM = 48, 12, 147212, 120
 PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv", "asm_keys", "asm_body",
-          "asm_contact", "asm_inverse", "dense", "swept", "energy_list", "ls_trials"]
+          "asm_contact", "asm_inverse", "dense", "swept", "energy_list", "ls_trials", "band"]
 
 
 class AbdError(RuntimeError):

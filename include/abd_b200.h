@@ -283,9 +283,10 @@ int abd_count_intersections(AbdHandle* h, int32_t* count);
  *   9 assembly: bodies          10 assembly: contacts     11 assembly: block inverse
  *   12 dense factor + solve     13 swept candidate list   14 contact-energy list kernel
  *   15 line-search trials (apply + energy + decision)
- * abd_get_timing writes ms[16], launches[16] and the algorithmic bytes[16]
+ *   16 banded block-Cholesky kernel of the direct solver
+ * abd_get_timing writes ms[17], launches[17] and the algorithmic bytes[17]
  * those phases moved (documented at each kernel); reset clears them. */
-#define ABD_NUM_PHASES 16
+#define ABD_NUM_PHASES 17
 int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset);
 int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes);
 
