@@ -54,7 +54,8 @@ class AbdParams(C.Structure):
         ("pinned_diag", C.c_double),
         ("warm_start", C.c_int32),
         ("broadphase", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("autotune", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

@@ -138,7 +138,6 @@ __global__ void __launch_bounds__(32 * BA_WARPS) k_body_assemble(int nb, const d
 // projected to PSD by the warp Jacobi (warp_eig.cuh), and scattered into the
 // body blocks: lanes own block entries, each summing the stencil vertices
 // that map to it through J = [1, xbar^T] (x) I3.
-#define CA_WARPS 4
 struct ContactSmem {
     WarpEigSmem E;
     double x[12], g[12], gy[9], aux[48], J[4][4];
@@ -282,16 +281,16 @@ DV void warp_distance_derivs(ContactSmem& C, const Geo& G) {
     __syncwarp();
 }
 
-template <class T>
-__global__ void __launch_bounds__(32 * CA_WARPS) k_contact_assemble(const Counters* cnt, const int4* __restrict__ cst,
+template <class T, int CAW>
+__global__ void __launch_bounds__(32 * CAW) k_contact_assemble(const Counters* cnt, const int4* __restrict__ cst,
                                    const int* __restrict__ ctype, const double* __restrict__ cxb, Geo G, int barrier,
                                    double dhat, double sc, int hess_mode, const int* __restrict__ row_ptr,
                                    const int* __restrict__ bcol, T* vals, double* grad) {
-    __shared__ ContactSmem sm[CA_WARPS];
+    __shared__ ContactSmem sm[CAW];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     ContactSmem& C = sm[w];
     const int n = cnt->n_total;
-    for (int c = blockIdx.x * CA_WARPS + w; c < n; c += gridDim.x * CA_WARPS) {
+    for (int c = blockIdx.x * CAW + w; c < n; c += gridDim.x * CAW) {
         int type = ctype[c];
         if (type < 0) continue;                       // warp-uniform
         if (lane == 0) {
@@ -462,6 +461,23 @@ int eng_sync_counters(Engine* E) {
 
 int eng_grow_blocks(Engine* E, int need);
 
+// the contact assembly with the autotuned number of warps per block
+template <class T>
+static void launch_contact_assemble(Engine* E, int n, Geo G, double sc, T* V) {
+    const AbdParams& P = E->P;
+    cudaStream_t s = E->stream;
+    int c = tune_begin(E, TK_CONTACT, 3, 1);
+    int w = TUNE_CONTACT_WARPS[c];
+    dim3 grid(grid_for(32L * n, 32 * w)), block(32 * w);
+    if (w == 2) k_contact_assemble<T, 2><<<grid, block, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
+                                                                P.hess_mode, E->row_ptr, E->bcol, V, E->g);
+    else if (w == 8) k_contact_assemble<T, 8><<<grid, block, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
+                                                                     P.hess_mode, E->row_ptr, E->bcol, V, E->g);
+    else k_contact_assemble<T, 4><<<grid, block, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
+                                                         P.hess_mode, E->row_ptr, E->bcol, V, E->g);
+    tune_end(E, TK_CONTACT);
+}
+
 int eng_assemble(Engine* E) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
@@ -498,8 +514,7 @@ int eng_assemble(Engine* E) {
                                                                P.k_ortho, P.hess_mode == ABD_HESS_PROJECTED, P.pinned_diag,
                                                                E->row_ptr, E->bcol, V, E->g);
         if (n > 0)
-            k_contact_assemble<float><<<grid_for(32L * n, 32 * CA_WARPS), 32 * CA_WARPS, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
-                                                                     P.hess_mode, E->row_ptr, E->bcol, V, E->g);
+            launch_contact_assemble<float>(E, n, G, sc, V);
         k_block_inverse<float><<<grid_for(32L * nb, 32 * BI_WARPS), 32 * BI_WARPS, 0, s>>>(nb, E->row_ptr, E->bcol, V, (float*)E->dinv);
     } else {
         double* V = (double*)E->vals;
@@ -511,8 +526,7 @@ int eng_assemble(Engine* E) {
         phase_end(E, p1, 0);
         int p2 = phase_begin(E, PH_ASM_CONTACT);
         if (n > 0)
-            k_contact_assemble<double><<<grid_for(32L * n, 32 * CA_WARPS), 32 * CA_WARPS, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
-                                                                      P.hess_mode, E->row_ptr, E->bcol, V, E->g);
+            launch_contact_assemble<double>(E, n, G, sc, V);
         // per candidate: type; per active contact: stencil, barrier argument,
         // 4 positions + 4 rest positions, 4 body blocks and the gradient rows
         phase_end(E, p2, 4.0 * n + E->hcnt->n_active * (16.0 + 8.0 + 96.0 + 96.0 + 4 * 1152.0 + 384.0));

@@ -141,6 +141,7 @@ int eng_alloc(Engine* E) {
 }
 
 void eng_free(Engine* E) {
+    for (auto& t : E->tune) { if (t.a) cudaEventDestroy(t.a); if (t.b) cudaEventDestroy(t.b); }
     eng_dense_free(E);
     eng_features_free(E);
     eng_mlp_free(E);
@@ -188,6 +189,7 @@ void abd_default_params(AbdParams* p) {
     p->precision = ABD_PREC_FP64;
     p->contact_capacity = 1 << 16;
     p->pinned_diag = 100.0;                       // abd.py:146
+    p->autotune = 1;
 }
 
 const char* abd_last_error(AbdHandle* h) {
@@ -554,6 +556,38 @@ static cudaEvent_t pool_get(Engine* E) {
     if (!E->ev_pool.empty()) { cudaEvent_t e = E->ev_pool.back(); E->ev_pool.pop_back(); return e; }
     cudaEvent_t e; cudaEventCreate(&e); return e;
 }
+int tune_begin(Engine* E, int k, int ncand, int dflt) {
+    Engine::Tuner& t = E->tune[k];
+    if (!E->P.autotune) return dflt;
+    if (t.chosen >= 0) return t.chosen;
+    if (!t.a) { cudaEventCreate(&t.a); cudaEventCreate(&t.b); }
+    if (t.running >= 0) {
+        float ms = 0;
+        if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+            t.sum[t.running] += ms; t.cnt[t.running]++;
+        }
+        t.running = -1;
+    }
+    int total = 0;
+    for (int c = 0; c < ncand; c++) total += t.cnt[c];
+    if (total >= ncand * TUNE_REPS) {
+        int best = dflt;
+        for (int c = 0; c < ncand; c++)
+            if (t.cnt[c] && t.sum[c] / t.cnt[c] < t.sum[best] / std::max(1, t.cnt[best])) best = c;
+        t.chosen = best;
+        return best;
+    }
+    int c = t.next;
+    t.next = (t.next + 1) % ncand;
+    t.running = c;
+    cudaEventRecord(t.a, E->stream);
+    return c;
+}
+void tune_end(Engine* E, int k) {
+    Engine::Tuner& t = E->tune[k];
+    if (t.running >= 0) cudaEventRecord(t.b, E->stream);
+}
+
 int phase_begin(Engine* E, int phase) {
     if (!E->timing) return -1;
     Engine::Rec r; r.phase = phase; r.a = pool_get(E); r.b = pool_get(E); r.bytes = 0;
@@ -585,6 +619,18 @@ extern "C" int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset) {
     if (reset) for (int i = 0; i < ABD_NUM_PHASES; i++) { E->phase_ms[i] = 0; E->phase_n[i] = 0; E->phase_bytes[i] = 0; }
     return ABD_OK;
 }
+extern "C" int abd_get_autotune(AbdHandle* h, int32_t* shapes, int32_t cap, int32_t* n) {
+    HANDLE(h);
+    if (!n || (cap > 0 && !shapes)) return E->fail(ABD_ERR_INVALID_ARG, "abd_get_autotune: null");
+    int v[TK_COUNT];
+    v[TK_CONTACT] = E->tune[TK_CONTACT].chosen < 0 ? -1 : TUNE_CONTACT_WARPS[E->tune[TK_CONTACT].chosen];
+    v[TK_LIST_ENERGY] = E->tune[TK_LIST_ENERGY].chosen < 0 ? -1 : TUNE_THREADS[E->tune[TK_LIST_ENERGY].chosen];
+    v[TK_BODY_ENERGY] = E->tune[TK_BODY_ENERGY].chosen < 0 ? -1 : TUNE_THREADS[E->tune[TK_BODY_ENERGY].chosen];
+    for (int i = 0; i < TK_COUNT && i < cap; i++) shapes[i] = v[i];
+    *n = TK_COUNT;
+    return ABD_OK;
+}
+
 extern "C" int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes) {
     HANDLE(h);
     cudaStreamSynchronize(E->stream);

@@ -542,8 +542,10 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
 // En (may be null) accumulates the scale of the FP64 evaluation error
 int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip) {
     const AbdParams& P = E->P;
-    k_body_energy<<<grid_for(E->nb), 256, 0, E->stream>>>(E->nb, E->st, E->mass, E->J, E->bscene, P.dt, P.gravity[0],
-                                                          P.gravity[1], P.gravity[2], P.k_ortho, skip, Eo, En);
+    int tb = TUNE_THREADS[tune_begin(E, TK_BODY_ENERGY, 4, 2)];
+    k_body_energy<<<grid_for(E->nb, tb), tb, 0, E->stream>>>(E->nb, E->st, E->mass, E->J, E->bscene, P.dt, P.gravity[0],
+                                                            P.gravity[1], P.gravity[2], P.k_ortho, skip, Eo, En);
+    tune_end(E, TK_BODY_ENERGY);
     E->launches++;
     return ABD_OK;
 }

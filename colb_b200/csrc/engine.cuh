@@ -105,6 +105,12 @@ struct Engine {
     std::string err;
     int launches = 0;
     int comp_band = 0, comp_small = 0, comp_large = 0, krylov_fallbacks = 0;   // direct-solver counters
+    struct Tuner {
+        int chosen = -1, next = 0, running = -1;
+        float sum[8] = {0}; int cnt[8] = {0};
+        cudaEvent_t a = nullptr, b = nullptr;
+    };
+    Tuner tune[3];
 
     // host-side scene offsets
     std::vector<int> h_body_begin, h_vert_begin, h_edge_begin, h_tri_begin, h_plane_begin;
@@ -229,6 +235,15 @@ DV int find_block(const int* row_ptr, const int* bcol, int r, int c) {
 #define GS_LOOP(i, n) for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (long)(n); i += (long)gridDim.x * blockDim.x)
 
 // implemented in the .cu files
+// launch-shape autotuner (capi.cu): tune_begin returns the candidate index to
+// launch (the chosen one once timed, the default when autotune is off) and
+// brackets it with events until every candidate was timed TUNE_REPS times
+enum { TK_CONTACT = 0, TK_LIST_ENERGY, TK_BODY_ENERGY, TK_COUNT };
+constexpr int TUNE_CONTACT_WARPS[3] = {2, 4, 8};            // default 4
+constexpr int TUNE_THREADS[4] = {64, 128, 256, 512};         // defaults 128 (list energy), 256 (body energy)
+constexpr int TUNE_REPS = 3;
+int tune_begin(Engine* E, int kernel, int ncand, int dflt);
+void tune_end(Engine* E, int kernel);
 int eng_alloc(Engine* E);
 void eng_free(Engine* E);
 int eng_transform(Engine* E);

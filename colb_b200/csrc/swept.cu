@@ -352,8 +352,10 @@ int eng_energy_list(Engine* E, int slot, const int* skip) {
     if ((rc = eng_body_energy(E, Eo, En, skip))) return rc;
     if (E->n_sw > 0) {
         int ph = phase_begin(E, PH_ELIST);
-        k_list_energy<<<grid_for(E->n_sw, 128), 128, 0, s>>>(E->n_sw, E->sw, eng_geo(E), E->bscene, skip, P.ee_f32, P.dhat,
-                                                             P.barrier, P.kappa * P.dt * P.dt, Eo, En);
+        int tb = TUNE_THREADS[tune_begin(E, TK_LIST_ENERGY, 4, 1)];
+        k_list_energy<<<grid_for(E->n_sw, tb), tb, 0, s>>>(E->n_sw, E->sw, eng_geo(E), E->bscene, skip, P.ee_f32, P.dhat,
+                                                           P.barrier, P.kappa * P.dt * P.dt, Eo, En);
+        tune_end(E, TK_LIST_ENERGY);
         // per listed pair: the entry, its 2-4 vertex ids and positions
         phase_end(E, ph, E->n_sw * (16.0 + 16.0 + 4 * 24.0));
         E->launches++;

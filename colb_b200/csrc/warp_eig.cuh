@@ -7,8 +7,11 @@
 // entries of A and every lane updates its share of the entries
 // independently.  n - 1 rounds (n even; odd n gets a dummy index) make one
 // sweep.  A rotation is skipped when |a_pq| is at rounding level against its
-// diagonal pair or against the whole matrix (rank-deficient Hessians drive
-// some diagonals to zero); sweeps stop when none was applied, the same
+// diagonal pair (1e-15 of their geometric mean) or against the whole matrix
+// (1e-14 of its Frobenius norm: rotations leave fill of about the rounding
+// unit times the norm, so a tighter floor would never be met on the barrier
+// Hessians' wide spectra, and rank-deficient Hessians drive some diagonals to
+// zero); sweeps stop when none was applied, the same
 // criterion the serial oracle uses.  The entry a rotation annihilates is set
 // to zero (not left at rounding level), so the sweeps end once the
 // off-diagonal mass has decayed.  A matrix whose Cholesky factorization
@@ -84,7 +87,7 @@ DV void warp_psd_project(WarpEigSmem& S, int n) {
                 double c = 1.0, s = 0.0;
                 if (q < n) {
                     double apq = S.A[p*12+q], app = S.A[p*12+p], aqq = S.A[q*12+q];
-                    if (fabs(apq) > fmax(1e-15 * sqrt(fabs(app * aqq)), 1e-16 * sqrt(fro))) {
+                    if (fabs(apq) > fmax(1e-15 * sqrt(fabs(app * aqq)), 1e-14 * sqrt(fro))) {
                         double theta = (aqq - app) / (2 * apq);
                         double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
                         c = rsqrt(t * t + 1); s = t * c;

@@ -23,6 +23,7 @@ EXPORTS = [
     "abd_count_intersections", "abd_last_error", "abd_abi_version", "abd_set_timing", "abd_get_timing",
     "abd_ee_pairs_static", "abd_set_mlp", "abd_mlp_forward", "abd_trainer_create", "abd_trainer_destroy",
     "abd_trainer_last_error", "abd_trainer_set_data", "abd_trainer_epoch", "abd_trainer_grad", "abd_trainer_params",
+    "abd_get_autotune",
 ]
 MLP_IN, MLP_OUT, MLP_NPARAM, MLP_NNORM = 48, 12, 147212, 120
 PHASES = ["detect", "assemble", "solve", "energy", "ccd", "other", "energy_query", "spmv", "asm_keys", "asm_body",
@@ -69,6 +70,7 @@ def load_library(path=LIB_PATH):
     L.abd_get_timing.argtypes = [vp, dp, C.POINTER(C.c_int64), dp]
     L.abd_ee_pairs_static.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_double, vp, C.c_int32, vp, vp]
     L.abd_set_mlp.argtypes = [vp, fp, fp]
+    L.abd_get_autotune.argtypes = [vp, ip, C.c_int32, ip]
     L.abd_mlp_forward.argtypes = [vp, fp, C.c_int32, fp]
     L.abd_trainer_create.argtypes = [C.c_int32, fp, C.POINTER(vp)]
     L.abd_trainer_destroy.argtypes = [vp]
@@ -215,6 +217,14 @@ class Engine:
         f = np.zeros((self.nb, 48), dtype=np.float32)
         self._check(self.L.abd_get_features(self.h, f.ctypes.data_as(C.POINTER(C.c_float)), self.nb))
         return f
+
+    def autotune(self):
+        """Launch shapes the autotuner chose (-1 while still timing):
+        contact-assembly warps per block, list-energy and body-energy threads."""
+        v = np.zeros(8, dtype=np.int32)
+        n = C.c_int32()
+        self._check(self.L.abd_get_autotune(self.h, _ip(v), 8, C.byref(n)))
+        return dict(zip(["contact_warps", "list_energy_threads", "body_energy_threads"], v[:n.value].tolist()))
 
     def set_timing(self, on=True, reset=True):
         self._check(self.L.abd_set_timing(self.h, int(on), int(reset)))

@@ -47,6 +47,7 @@ REFERENCE = dict(
     contact_capacity=1 << 16,
     pinned_diag=100.0,
     warm_start=0,
+    autotune=1,
 )
 
 CONFIG = dict(
@@ -74,6 +75,7 @@ CONFIG = dict(
     contact_capacity=1 << 20,
     pinned_diag=100.0,
     warm_start=0,
+    autotune=1,
 )
 
 

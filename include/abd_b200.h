@@ -107,7 +107,10 @@ typedef struct AbdParams {
                                (abd_set_mlp); 1, 2 and 3 are clipped by CCD */
     int32_t broadphase;     /* 0 auto, 1 hashed grid over primitives, 2 body pairs then primitives
                                (needs contiguous per-body vertex/edge/triangle ranges) */
-    int32_t reserved[6];
+    int32_t autotune;       /* 1: time the launch-shape candidates of the tunable kernels during
+                               the first Newton iterations of the handle and keep the fastest
+                               (abd_get_autotune); 0: fixed launch shapes */
+    int32_t reserved[5];
 } AbdParams;
 
 /* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */
@@ -269,6 +272,12 @@ int abd_trainer_epoch(AbdTrainer* t, const int32_t* order, int32_t n, int32_t ba
 /* Loss and gradient (ABD_MLP_NPARAM floats) on the given rows, no update. */
 int abd_trainer_grad(AbdTrainer* t, const float* x, const float* y, int32_t n, float* grad, float* loss);
 int abd_trainer_params(AbdTrainer* t, float* params);
+
+/* Launch shapes chosen by the autotuner (no reference counterpart), one per
+ * tunable kernel: [0] warps per block of the contact assembly, [1] threads per
+ * block of the listed-pair energy, [2] threads per block of the body energy;
+ * -1 while still timing candidates.  *n gets the number of tunable kernels. */
+int abd_get_autotune(AbdHandle* h, int32_t* shapes, int32_t cap, int32_t* n);
 
 /* Number of edge-triangle intersections between different bodies at the
  * nxt state (FP64 exact predicate); 0 means intersection-free. */

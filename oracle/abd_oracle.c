@@ -356,13 +356,14 @@ void oracle_psd_project(int n, double* H) {
     double fro = 0; for (int i = 0; i < n*n; i++) fro += A[i]*A[i];
     if (fro == 0) return;
     /* a rotation is skipped when |a_pq| is at rounding level against its
-     * diagonal pair or against the whole matrix; the sweeps stop when none
-     * was applied (scale-invariant) */
+     * diagonal pair (1e-15 of their geometric mean) or against the whole
+     * matrix (1e-14 of its Frobenius norm, above the fill rotations leave);
+     * the sweeps stop when none was applied (scale-invariant) */
     for (int sweep = 0; sweep < 50; sweep++) {
         int rotated = 0;
         for (int p = 0; p < n; p++) for (int q = p + 1; q < n; q++) {
             double apq = A[p*n+q];
-            if (fabs(apq) <= fmax(1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])), 1e-16 * sqrt(fro))) continue;
+            if (fabs(apq) <= fmax(1e-15 * sqrt(fabs(A[p*n+p] * A[q*n+q])), 1e-14 * sqrt(fro))) continue;
             rotated = 1;
             double theta = (A[q*n+q] - A[p*n+p]) / (2 * apq);
             double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta*theta + 1));

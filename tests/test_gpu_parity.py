@@ -173,6 +173,23 @@ def test_warm_start_trajectory_matches_oracle(warm_start):
         assert e.count_intersections() == 0
 
 
+def test_autotuner_picks_listed_launch_shapes():
+    """The autotuner times every candidate launch shape during the first
+    iterations, keeps the fastest, and the trajectory still matches the oracle."""
+    sc = S.config2_chain_net(n=3, pitch=1.5 - 5e-4, seed=2)
+    p = P.config_params(dt=1.0 / 240.0, autotune=1)
+    e, o = _pair(p, sc)
+    e.step(3); o.step(3)
+    tuned = e.autotune()
+    assert tuned["contact_warps"] in (2, 4, 8)
+    assert tuned["list_energy_threads"] in (64, 128, 256, 512)
+    assert tuned["body_energy_threads"] in (64, 128, 256, 512)
+    assert np.abs(e.vertices() - o.vertices()).max() <= 1e-6 * np.abs(o.vertices()).max()
+    off = Engine(P.config_params(dt=1.0 / 240.0, autotune=0), sc)
+    off.step(1)
+    assert off.autotune() == {"contact_warps": -1, "list_energy_threads": -1, "body_energy_threads": -1}
+
+
 def test_batch_equals_single_scenes():
     scenes = S.config3_batch(n_scenes=4, seed=7, nmin=4, nmax=8)
     p = P.config_params(lin_tol=1e-10)
