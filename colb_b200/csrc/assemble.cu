@@ -384,6 +384,112 @@ __global__ void __launch_bounds__(32 * CAW) k_contact_assemble(const Counters* c
     }
 }
 
+// One block of NT threads per active contact: the same work as
+// k_contact_assemble, with the PSD projection spread over the whole block.
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_contact_assemble_team(const Counters* cnt, const int4* __restrict__ cst,
+                                   const int* __restrict__ ctype, const double* __restrict__ cxb, Geo G, int barrier,
+                                   double dhat, double sc, int hess_mode, const int* __restrict__ row_ptr,
+                                   const int* __restrict__ bcol, T* vals, double* grad) {
+    __shared__ ContactSmem C;
+    const int tid = threadIdx.x, warp = threadIdx.x >> 5;
+    const int n = cnt->n_total;
+    for (int c = blockIdx.x; c < n; c += gridDim.x) {
+        int type = ctype[c];
+        if (type < 0) continue;                       // block-uniform
+        if (tid == 0) {
+            int4 s4 = cst[c];
+            int sv[4] = {s4.x, s4.y, s4.z, s4.w};
+            C.type = type;
+            C.np = stencil_np(type);
+            for (int i = 0; i < 4; i++) C.v[i] = sv[i];
+            int nx = type == T_PG ? 1 : C.np;
+            for (int i = 0; i < nx; i++) {
+                int v = sv[i];
+                for (int k = 0; k < 3; k++) C.x[3*i+k] = G.x[3*v+k];
+                C.vb[i] = G.vbody[v];
+                C.J[i][0] = 1.0; C.J[i][1] = G.xbar[3*v]; C.J[i][2] = G.xbar[3*v+1]; C.J[i][3] = G.xbar[3*v+2];
+            }
+            barrier3(barrier, cxb[c], dhat * dhat, C.B0, C.B1, C.B2);
+            C.bodies[0] = C.vb[0]; C.nbd = 1;
+            for (int i = 1; i < C.np; i++) if (C.vb[i] != C.bodies[0]) { C.bodies[1] = C.vb[i]; C.nbd = 2; break; }
+        }
+        __syncthreads();
+        if (warp == 0) warp_distance_derivs(C, G);
+        __syncthreads();
+        const int np = C.np, m = 3 * np;
+        const double B1 = C.B1, B2 = C.B2;
+        double* A = C.E.A;
+        if (hess_mode == ABD_HESS_REFERENCE) {
+            if (C.type == T_EE) team_psd_project<NT>(C.E, 12);               // abd.py:247
+            for (int e = tid; e < m * m; e += NT) {
+                int i = e / m, j = e % m;
+                double h = (C.type == T_PP) ? 0.0 : B1 * A[i*12+j];       // abd.py:381-382
+                A[i*12+j] = (h + B2 * C.g[i] * C.g[j]) * sc;
+            }
+            __syncthreads();
+        } else if (C.type == T_PG || C.type == T_PP) {
+            // analytic projection.  With d the separation (g = 2d on the first
+            // point), B1 H + B2 g g^T is [M] (point-plane, d along the normal)
+            // or [M -M; -M M] (point-point) with M = 2 B1 I + 4 B2 d d^T for
+            // point-point and M = (2 B1 + 4 B2 d^2) n n^T for point-plane; the
+            // projection clamps M's eigenvalues 2 B1 (across d) and
+            // 2 B1 + 4 B2 |d|^2 (along d) at zero.
+            const double dx = 0.5 * C.g[0], dy = 0.5 * C.g[1], dz = 0.5 * C.g[2];
+            const double dd = dx * dx + dy * dy + dz * dz;
+            const double lam_t = C.type == T_PP ? fmax(2.0 * B1, 0.0) : 0.0;
+            const double lam_n = fmax(2.0 * B1 + 4.0 * B2 * dd, 0.0);
+            const double dv[3] = {dx, dy, dz};
+            for (int e = tid; e < m * m; e += NT) {
+                int i = e / m, j = e % m, a = i % 3, b = j % 3;
+                double nn = dd > 0.0 ? dv[a] * dv[b] / dd : 0.0;
+                double Mab = lam_t * ((a == b ? 1.0 : 0.0) - nn) + lam_n * nn;
+                A[i*12+j] = ((i / 3) == (j / 3) ? Mab : -Mab) * sc;
+            }
+            __syncthreads();
+        } else {
+            for (int e = tid; e < m * m; e += NT) {
+                int i = e / m, j = e % m;
+                A[i*12+j] = B1 * A[i*12+j] + B2 * C.g[i] * C.g[j];
+            }
+            __syncthreads();
+            team_psd_project<NT>(C.E, m);
+            for (int e = tid; e < m * m; e += NT) { int i = e / m, j = e % m; A[i*12+j] *= sc; }
+            __syncthreads();
+        }
+        // gradient: G[b][3 al + k] += J_i[al] g_i[k] * B1 * sc for dynamic bodies
+        for (int e = tid; e < np * 12; e += NT) {
+            int i = e / 12, al = (e % 12) / 3, k = e % 3;
+            int b = C.vb[i];
+            if (G.mass[b] > 0.0) atomicAdd(grad + 12L * b + 3 * al + k, C.J[i][al] * C.g[3*i+k] * B1 * sc);
+        }
+        // Hessian blocks of the (at most two) bodies
+        for (int pa = 0; pa < C.nbd; pa++)
+            for (int pb = 0; pb < C.nbd; pb++) {
+                int Ba = C.bodies[pa], Bb = C.bodies[pb];
+                if (!(G.mass[Ba] > 0.0) || !(G.mass[Bb] > 0.0)) continue;
+                int bi = find_block(row_ptr, bcol, Ba, Bb);
+                if (bi < 0) continue;
+                T* V = vals + (long)bi * 144;
+                for (int e = tid; e < 144; e += NT) {
+                    int row = e % 12, col = e / 12;          // column-major block entry (row, col)
+                    int al = row / 3, r = row % 3, be = col / 3, q = col % 3;
+                    double sum = 0;
+                    for (int i = 0; i < np; i++) {
+                        if (C.vb[i] != Ba) continue;
+                        for (int j = 0; j < np; j++) {
+                            if (C.vb[j] != Bb) continue;
+                            sum += C.J[i][al] * C.J[j][be] * A[(3*i+r)*12 + 3*j+q];
+                        }
+                    }
+                    if (sum != 0.0) atomicAdd(V + e, (T)sum);
+                }
+            }
+        __syncthreads();
+    }
+}
+
+
 // ---------------------------------------------------- block-Jacobi inverse
 // One warp per body: Gauss-Jordan with partial pivoting on [D | I] in shared
 // memory, lanes owning the 24 columns.  A singular block gives the identity.
@@ -461,20 +567,23 @@ int eng_sync_counters(Engine* E) {
 
 int eng_grow_blocks(Engine* E, int need);
 
-// the contact assembly with the autotuned number of warps per block
+// the contact assembly with the autotuned launch shape: one warp per
+// contact (2, 4 or 8 contacts per block) or one block of 64 / 128 threads per
+// contact
 template <class T>
 static void launch_contact_assemble(Engine* E, int n, Geo G, double sc, T* V) {
     const AbdParams& P = E->P;
     cudaStream_t s = E->stream;
-    int c = tune_begin(E, TK_CONTACT, 3, 1);
-    int w = TUNE_CONTACT_WARPS[c];
-    dim3 grid(grid_for(32L * n, 32 * w)), block(32 * w);
-    if (w == 2) k_contact_assemble<T, 2><<<grid, block, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
-                                                                P.hess_mode, E->row_ptr, E->bcol, V, E->g);
-    else if (w == 8) k_contact_assemble<T, 8><<<grid, block, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
-                                                                     P.hess_mode, E->row_ptr, E->bcol, V, E->g);
-    else k_contact_assemble<T, 4><<<grid, block, 0, s>>>(E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc,
-                                                         P.hess_mode, E->row_ptr, E->bcol, V, E->g);
+    int c = tune_begin(E, TK_CONTACT, 5, 1);
+    const int threads = TUNE_CONTACT_THREADS[c], per_block = TUNE_CONTACT_PER_BLOCK[c];
+    dim3 block(threads), grid(grid_for((long)n, per_block));
+#define CA_ARGS E->dcnt, E->cst, E->ctype, E->cxb, G, P.barrier, P.dhat, sc, P.hess_mode, E->row_ptr, E->bcol, V, E->g
+    if (c == 0) k_contact_assemble<T, 2><<<grid, block, 0, s>>>(CA_ARGS);
+    else if (c == 2) k_contact_assemble<T, 8><<<grid, block, 0, s>>>(CA_ARGS);
+    else if (c == 3) k_contact_assemble_team<T, 64><<<grid, block, 0, s>>>(CA_ARGS);
+    else if (c == 4) k_contact_assemble_team<T, 128><<<grid, block, 0, s>>>(CA_ARGS);
+    else k_contact_assemble<T, 4><<<grid, block, 0, s>>>(CA_ARGS);
+#undef CA_ARGS
     tune_end(E, TK_CONTACT);
 }
 

@@ -622,12 +622,14 @@ extern "C" int abd_set_timing(AbdHandle* h, int32_t on, int32_t reset) {
 extern "C" int abd_get_autotune(AbdHandle* h, int32_t* shapes, int32_t cap, int32_t* n) {
     HANDLE(h);
     if (!n || (cap > 0 && !shapes)) return E->fail(ABD_ERR_INVALID_ARG, "abd_get_autotune: null");
-    int v[TK_COUNT];
-    v[TK_CONTACT] = E->tune[TK_CONTACT].chosen < 0 ? -1 : TUNE_CONTACT_WARPS[E->tune[TK_CONTACT].chosen];
-    v[TK_LIST_ENERGY] = E->tune[TK_LIST_ENERGY].chosen < 0 ? -1 : TUNE_THREADS[E->tune[TK_LIST_ENERGY].chosen];
-    v[TK_BODY_ENERGY] = E->tune[TK_BODY_ENERGY].chosen < 0 ? -1 : TUNE_THREADS[E->tune[TK_BODY_ENERGY].chosen];
-    for (int i = 0; i < TK_COUNT && i < cap; i++) shapes[i] = v[i];
-    *n = TK_COUNT;
+    int v[4];
+    int cc = E->tune[TK_CONTACT].chosen;
+    v[0] = cc < 0 ? -1 : TUNE_CONTACT_THREADS[cc];
+    v[1] = cc < 0 ? -1 : TUNE_CONTACT_PER_BLOCK[cc];
+    v[2] = E->tune[TK_LIST_ENERGY].chosen < 0 ? -1 : TUNE_THREADS[E->tune[TK_LIST_ENERGY].chosen];
+    v[3] = E->tune[TK_BODY_ENERGY].chosen < 0 ? -1 : TUNE_THREADS[E->tune[TK_BODY_ENERGY].chosen];
+    for (int i = 0; i < 4 && i < cap; i++) shapes[i] = v[i];
+    *n = 4;
     return ABD_OK;
 }
 

@@ -239,7 +239,10 @@ DV int find_block(const int* row_ptr, const int* bcol, int r, int c) {
 // launch (the chosen one once timed, the default when autotune is off) and
 // brackets it with events until every candidate was timed TUNE_REPS times
 enum { TK_CONTACT = 0, TK_LIST_ENERGY, TK_BODY_ENERGY, TK_COUNT };
-constexpr int TUNE_CONTACT_WARPS[3] = {2, 4, 8};            // default 4
+// contact assembly: one warp per contact with 2, 4 (default) or 8 per block,
+// or one block of 64 or 128 threads per contact
+constexpr int TUNE_CONTACT_THREADS[5] = {64, 128, 256, 64, 128};
+constexpr int TUNE_CONTACT_PER_BLOCK[5] = {2, 4, 8, 1, 1};
 constexpr int TUNE_THREADS[4] = {64, 128, 256, 512};         // defaults 128 (list energy), 256 (body energy)
 constexpr int TUNE_REPS = 3;
 int tune_begin(Engine* E, int kernel, int ncand, int dflt);

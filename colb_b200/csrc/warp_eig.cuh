@@ -28,6 +28,7 @@ struct WarpEigSmem {
     int role[12];        // 0: index is p of its pair, 1: index is q
     int pair_of[12];
     int flag;
+    double red[4];       // per-warp partial sums of a team of up to 128 threads
 };
 
 // pairs of round r in a tournament of m players (m even): player m-1 fixed,
@@ -41,69 +42,80 @@ DV void tournament_pair(int m, int r, int k, int& p, int& q) {
     if (p > q) { int t = p; p = q; q = t; }
 }
 
-// Cholesky of S.A into S.T (lanes own rows): true when every pivot is
-// positive, i.e. S.A is positive definite and its own PSD projection.
-DV bool warp_is_pd(WarpEigSmem& S, int n) {
-    const int lane = threadIdx.x & 31;
-    for (int e = lane; e < 144; e += 32) S.T[e] = S.A[e];
-    __syncwarp();
+template <int NT> DV void team_sync() { if (NT > 32) __syncthreads(); else __syncwarp(); }
+
+// Cholesky of S.A into S.T (threads own rows): true when every pivot is
+// positive, i.e. S.A is positive definite and its own PSD projection.  A team
+// is one warp (NT = 32) or a whole block of NT threads.
+template <int NT>
+DV bool team_is_pd(WarpEigSmem& S, int n) {
+    const int t = threadIdx.x % NT;
+    for (int e = t; e < 144; e += NT) S.T[e] = S.A[e];
+    team_sync<NT>();
     bool ok = true;
     for (int k = 0; k < n; k++) {
-        double d = S.T[k*12+k];                 // same value in every lane
+        double d = S.T[k*12+k];                 // same value in every thread
         if (!(d > 0.0)) { ok = false; break; }
         d = sqrt(d);
-        if (lane > k && lane < n) S.T[lane*12+k] /= d;
-        __syncwarp();
-        if (lane > k && lane < n) {
-            double lik = S.T[lane*12+k];
-            for (int j = k + 1; j <= lane; j++) S.T[lane*12+j] -= lik * S.T[j*12+k];
+        if (t > k && t < n) S.T[t*12+k] /= d;
+        team_sync<NT>();
+        if (t > k && t < n) {
+            double lik = S.T[t*12+k];
+            for (int j = k + 1; j <= t; j++) S.T[t*12+j] -= lik * S.T[j*12+k];
         }
-        __syncwarp();
+        team_sync<NT>();
     }
-    __syncwarp();
+    team_sync<NT>();
     return ok;
 }
 
-// Project S.A (n x n, ld 12) in place.  All 32 lanes call it.  A positive
-// definite matrix is returned unchanged.
-DV void warp_psd_project(WarpEigSmem& S, int n) {
-    const int lane = threadIdx.x & 31;
+// Project S.A (n x n, ld 12) in place.  All NT threads of the team call it.
+// A positive definite matrix is returned unchanged.
+template <int NT>
+DV void team_psd_project(WarpEigSmem& S, int n) {
+    const int t = threadIdx.x % NT, lane = threadIdx.x & 31;
     const int m = (n & 1) ? n + 1 : n;      // players, index n is a dummy when n is odd
-    for (int e = lane; e < 144; e += 32) { int i = e / 12, j = e % 12; S.V[e] = (i == j) ? 1.0 : 0.0; }
-    // scale for the all-zero test
+    for (int e = t; e < 144; e += NT) { int i = e / 12, j = e % 12; S.V[e] = (i == j) ? 1.0 : 0.0; }
+    // scale for the all-zero test and the rotation floor
     double fro = 0;
-    for (int e = lane; e < n * n; e += 32) { int i = e / n, j = e % n; fro += S.A[i*12+j] * S.A[i*12+j]; }
+    for (int e = t; e < n * n; e += NT) { int i = e / n, j = e % n; fro += S.A[i*12+j] * S.A[i*12+j]; }
     for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+    if (NT > 32) {
+        if (lane == 0) S.red[t >> 5] = fro;
+        team_sync<NT>();
+        fro = 0;
+        for (int w = 0; w < NT / 32; w++) fro += S.red[w];
+    }
     if (fro == 0.0) return;
-    __syncwarp();
-    if (warp_is_pd(S, n)) return;
+    team_sync<NT>();
+    if (team_is_pd<NT>(S, n)) return;
     for (int sweep = 0; sweep < 50; sweep++) {
-        if (lane == 0) S.flag = 0;
-        __syncwarp();
+        if (t == 0) S.flag = 0;
+        team_sync<NT>();
         for (int r = 0; r < m - 1; r++) {
             // rotation angles of this round's pairs
-            if (lane < m / 2) {
-                int p, q; tournament_pair(m, r, lane, p, q);
+            if (t < m / 2) {
+                int p, q; tournament_pair(m, r, t, p, q);
                 double c = 1.0, s = 0.0;
                 if (q < n) {
                     double apq = S.A[p*12+q], app = S.A[p*12+p], aqq = S.A[q*12+q];
                     if (fabs(apq) > fmax(1e-15 * sqrt(fabs(app * aqq)), 1e-14 * sqrt(fro))) {
                         double theta = (aqq - app) / (2 * apq);
-                        double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-                        c = rsqrt(t * t + 1); s = t * c;
+                        double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+                        c = rsqrt(tt * tt + 1); s = tt * c;
                         S.flag = 1;
                     }
                     S.partner[p] = q; S.partner[q] = p; S.role[p] = 0; S.role[q] = 1;
-                    S.pair_of[p] = lane; S.pair_of[q] = lane;
+                    S.pair_of[p] = t; S.pair_of[q] = t;
                 } else if (p < n) {
                     S.partner[p] = -1;
                 }
-                S.c[lane] = c; S.s[lane] = s;
+                S.c[t] = c; S.s[t] = s;
             }
-            __syncwarp();
+            team_sync<NT>();
             // column j of R: R[j][j] = c, R[partner][j] = -s if j is p, +s if j is q.
             // pass 1: T = R^T A R; every entry reads at most four entries of A
-            for (int e = lane; e < n * n; e += 32) {
+            for (int e = t; e < n * n; e += NT) {
                 int i = e / n, j = e % n;
                 int pi = S.partner[i], pj = S.partner[j];
                 double ci = 1, si = 0, cj = 1, sj = 0;
@@ -117,9 +129,9 @@ DV void warp_psd_project(WarpEigSmem& S, int n) {
                 if (pj == i && S.s[S.pair_of[i]] != 0.0) v = 0.0;
                 S.T[i*12+j] = v;
             }
-            __syncwarp();
+            team_sync<NT>();
             // pass 2: V R into A (free now that T holds the rotated matrix)
-            for (int e = lane; e < n * n; e += 32) {
+            for (int e = t; e < n * n; e += NT) {
                 int i = e / n, j = e % n;
                 int pj = S.partner[j];
                 double cj = 1, sj = 0;
@@ -128,30 +140,33 @@ DV void warp_psd_project(WarpEigSmem& S, int n) {
                 if (pj >= 0) w += sj * S.V[i*12+pj];
                 S.A[i*12+j] = w;
             }
-            __syncwarp();
+            team_sync<NT>();
             // pass 3: swap back
-            for (int e = lane; e < n * n; e += 32) {
+            for (int e = t; e < n * n; e += NT) {
                 int i = e / n, j = e % n;
                 double a = S.T[i*12+j], v = S.A[i*12+j];
                 S.V[i*12+j] = v;
                 S.A[i*12+j] = a;
             }
-            __syncwarp();
-            if (lane < 12) { S.partner[lane] = -1; }
-            __syncwarp();
+            team_sync<NT>();
+            if (t < 12) { S.partner[t] = -1; }
+            team_sync<NT>();
         }
         if (!S.flag) break;
-        __syncwarp();
+        team_sync<NT>();
     }
-    __syncwarp();
+    team_sync<NT>();
     // H = V max(L,0) V^T into T, then back into A
-    for (int e = lane; e < n * n; e += 32) {
+    for (int e = t; e < n * n; e += NT) {
         int i = e / n, j = e % n;
         double acc = 0;
         for (int k = 0; k < n; k++) { double l = S.A[k*12+k]; if (l > 0) acc += S.V[i*12+k] * l * S.V[j*12+k]; }
         S.T[i*12+j] = acc;
     }
-    __syncwarp();
-    for (int e = lane; e < n * n; e += 32) { int i = e / n, j = e % n; S.A[i*12+j] = S.T[i*12+j]; }
-    __syncwarp();
+    team_sync<NT>();
+    for (int e = t; e < n * n; e += NT) { int i = e / n, j = e % n; S.A[i*12+j] = S.T[i*12+j]; }
+    team_sync<NT>();
 }
+
+DV bool warp_is_pd(WarpEigSmem& S, int n) { return team_is_pd<32>(S, n); }
+DV void warp_psd_project(WarpEigSmem& S, int n) { team_psd_project<32>(S, n); }

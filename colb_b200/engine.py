@@ -219,12 +219,14 @@ class Engine:
         return f
 
     def autotune(self):
-        """Launch shapes the autotuner chose (-1 while still timing):
-        contact-assembly warps per block, list-energy and body-energy threads."""
+        """Launch shapes the autotuner chose (-1 while still timing): contact
+        assembly threads and contacts per block, list-energy and body-energy
+        threads per block."""
         v = np.zeros(8, dtype=np.int32)
         n = C.c_int32()
         self._check(self.L.abd_get_autotune(self.h, _ip(v), 8, C.byref(n)))
-        return dict(zip(["contact_warps", "list_energy_threads", "body_energy_threads"], v[:n.value].tolist()))
+        return dict(zip(["contact_threads", "contacts_per_block", "list_energy_threads", "body_energy_threads"],
+                        v[:n.value].tolist()))
 
     def set_timing(self, on=True, reset=True):
         self._check(self.L.abd_set_timing(self.h, int(on), int(reset)))

@@ -273,10 +273,11 @@ int abd_trainer_epoch(AbdTrainer* t, const int32_t* order, int32_t n, int32_t ba
 int abd_trainer_grad(AbdTrainer* t, const float* x, const float* y, int32_t n, float* grad, float* loss);
 int abd_trainer_params(AbdTrainer* t, float* params);
 
-/* Launch shapes chosen by the autotuner (no reference counterpart), one per
- * tunable kernel: [0] warps per block of the contact assembly, [1] threads per
- * block of the listed-pair energy, [2] threads per block of the body energy;
- * -1 while still timing candidates.  *n gets the number of tunable kernels. */
+/* Launch shapes chosen by the autotuner (no reference counterpart): [0]
+ * threads per block and [1] contacts per block of the contact assembly (one
+ * warp per contact, or one block of 64 / 128 threads per contact), [2]
+ * threads per block of the listed-pair energy, [3] of the body energy; -1
+ * while still timing candidates.  *n gets the number of entries (4). */
 int abd_get_autotune(AbdHandle* h, int32_t* shapes, int32_t cap, int32_t* n);
 
 /* Number of edge-triangle intersections between different bodies at the

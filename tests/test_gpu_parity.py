@@ -181,13 +181,13 @@ def test_autotuner_picks_listed_launch_shapes():
     e, o = _pair(p, sc)
     e.step(3); o.step(3)
     tuned = e.autotune()
-    assert tuned["contact_warps"] in (2, 4, 8)
+    assert (tuned["contact_threads"], tuned["contacts_per_block"]) in [(64, 2), (128, 4), (256, 8), (64, 1), (128, 1)]
     assert tuned["list_energy_threads"] in (64, 128, 256, 512)
     assert tuned["body_energy_threads"] in (64, 128, 256, 512)
     assert np.abs(e.vertices() - o.vertices()).max() <= 1e-6 * np.abs(o.vertices()).max()
     off = Engine(P.config_params(dt=1.0 / 240.0, autotune=0), sc)
     off.step(1)
-    assert off.autotune() == {"contact_warps": -1, "list_energy_threads": -1, "body_energy_threads": -1}
+    assert set(off.autotune().values()) == {-1}
 
 
 def test_batch_equals_single_scenes():
