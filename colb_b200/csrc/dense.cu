@@ -280,7 +280,7 @@ constexpr int BAND_W = BAND_MAX + 1;
 constexpr int BAND_THREADS = 256;
 
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
-constexpr int BAND_PREFER_MAX = 24;    // above this many bodies cuSOLVER is preferred while it has room
+constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
 
 // 1/sqrt(d): a single-precision estimate refined by two Newton-Raphson steps
 // r <- r (3 - d r^2) / 2 (each squares the relative error: 2^-23 -> 2^-46 ->
@@ -375,10 +375,11 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     T l = a[j] * r;                          // L[lane][j] for lane > j
                     if (lane == j) a[j] = d * r;
                     if (lane > j) a[j] = l;
+                    // full-range inner loop: every index static, so a[] stays in registers
 #pragma unroll
-                    for (int c2 = j + 1; c2 < 12; c2++) {
-                        T lc = __shfl_sync(0xffffffffu, l, c2);   // L[c2][j]
-                        if (lane > j) a[c2] -= l * lc;
+                    for (int c2 = 0; c2 < 12; c2++) {
+                        T lc = __shfl_sync(0xffffffffu, l, c2);   // L[c2][j] for c2 > j
+                        if (c2 > j && lane > j) a[c2] -= l * lc;
                     }
                 }
                 if (lane < 12) {
