@@ -2,6 +2,8 @@
 iterations per step) for one workload, as one JSON line.
 
 Workloads (--workload):
+  pile    4096 icospheres landing in a 12x12x40 open box, dt = 1/120, from
+          the state after 100 steps (the dense pile-up configuration)
   net16   16x16 chain mail of 256 torus links (288 verts / 576 tris each),
           corner links pinned, dt = 1/240, FP64 (default; the chain-net
           configuration of the benchmark suite)
@@ -35,6 +37,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "ABD body-steps/s @1e-5 residual: learned+batched vs plain, same B200; iters/step"
+PILE_MAX_ITER = 512
 
 
 def make_workload(name, rank=0, precision=0, ns_batch=512, world=1):
@@ -48,6 +51,19 @@ def make_workload(name, rank=0, precision=0, ns_batch=512, world=1):
                    f"4 corners pinned, dt 1/240, log barrier dhat 1e-3 kappa 1e7, k_ortho 1e7, CCD line search; "
                    f"timed from the resting state after {t0} plain FP64 steps (colb_b200/data/net16_t120.npz)",
                    bodies=256, verts=len(sc["xbar"]), tris=len(sc["tris"]), start_step=t0)
+        return [sc], p, cfg
+    if name == "pile":
+        from colb_b200 import fixtures
+        state, t0, seed = fixtures.load_pile()
+        sc = dict(S.config5_pile(seed=seed), state=state)
+        # landing spheres need far more than 64 Newton iterations per step
+        # to reach the 1e-5 residual (the cap ends the step unconverged)
+        p = P.config_params(precision=precision, newton_max_iter=PILE_MAX_ITER)
+        cfg = dict(workload=f"pile: 4096 icospheres (subdivision 1/2, r U(0.2,0.5)) dropped into a 12x12x40 open box "
+                   f"(ground + 4 wall half-spaces), dt 1/120, log barrier dhat 1e-3 kappa 1e7, k_ortho 1e7, CCD line "
+                   f"search, Newton cap {PILE_MAX_ITER}; timed from step {t0} while the spheres land "
+                   f"(colb_b200/data/pile_t100.npz)", bodies=4096, verts=len(sc["xbar"]), tris=len(sc["tris"]),
+                   start_step=t0)
         return [sc], p, cfg
     if name == "net16c":
         sc = S.config2_chain_net(n=16, seed=rank, pitch=1.5 - 5e-4)
@@ -205,6 +221,9 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     scenes, p, cfg = make_workload(args.workload, rank, args.precision, world=world)
+    if args.ls_groups:
+        p.ls_groups = 1
+        cfg = dict(cfg, line_search="one step length per contact group")
     if args.warm_start:
         p.warm_start = args.warm_start
         cfg = dict(cfg, warm_start={2: "inertial", 3: "learned (colb_b200/data/warmstart_net16.npz)"}[args.warm_start])
@@ -293,6 +312,12 @@ def run_forms(args, scenes, p, dev=0):
     base = params_to_dict(p)
     forms = {"mixed": (dict(precision=1), 1, False), "learned": (dict(warm_start=3), 1, True),
              "batched_x8": ({}, 8, False), "learned+batched_x8+mixed": (dict(precision=1, warm_start=3), 8, True)}
+    if args.workload == "pile":
+        # one scene of 4096 bodies: the batched form steps its contact groups
+        # as independent units (one step length per group, ls_groups)
+        forms = {"mixed": (dict(precision=1), 1, False), "contact_groups": (dict(ls_groups=1), 1, False),
+                 "learned": (dict(warm_start=3), 1, True),
+                 "learned+contact_groups+mixed": (dict(precision=1, warm_start=3, ls_groups=1), 1, True)}
     out = {}
     for name, (over, copies, learned) in forms.items():
         e = None
@@ -326,7 +351,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="net16", choices=["net16", "net16c", "chain", "cubes", "batch"])
+    ap.add_argument("--workload", default="net16", choices=["net16", "net16c", "chain", "cubes", "batch", "pile"])
+    ap.add_argument("--ls-groups", type=int, default=0, choices=[0, 1], help="1: one step length per contact group")
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed FP32/FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warm-start", type=int, default=0, choices=[0, 2, 3], help="0 plain, 2 inertial, 3 learned network")
@@ -339,6 +365,10 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            return
+        if args.workload == "pile":
+            print(json.dumps({"impl": "reference", "metric": METRIC,
+                              "unavailable": "one CPU oracle step of the 4096-body pile takes longer than 15 min on 8 cores"}))
             return
         scenes, p, cfg = make_workload(args.workload, 0, args.precision)
         cb = cpu_baseline(scenes, p, cfg, budget_s=max(10.0, 6.0 * args.steps))
@@ -399,13 +429,18 @@ def main():
         "phases_ms_per_step": {k: v["ms"] / r["n_timing"] for k, v in ph.items()},
         "clocks": r["clocks"],
     }
-    if rank == 0 and world == 1 and args.workload == "net16" and not args.no_forms:
+    if rank == 0 and world == 1 and args.workload in ("net16", "pile") and not args.no_forms:
         forms = {"plain_fp64": {"value": value, "unit": "body-steps/s",
                                 "newton_iters_per_step": line["newton_iters_per_step"], "steps": args.steps}}
         forms.update(run_forms(args, r["scenes"], r["p"]))
         line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(r["scenes"], r["p"], r["cfg"])
+        if args.workload == "pile":
+            line["cpu_baseline"] = {"value": None, "unit": "body-steps/s", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": "none: one oracle step of the 4096-body pile takes longer than 15 min on "
+                                              "8 host cores, beyond a bounded sample"}
+        else:
+            line["cpu_baseline"] = cpu_baseline(r["scenes"], r["p"], r["cfg"])
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

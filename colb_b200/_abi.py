@@ -55,7 +55,8 @@ class AbdParams(C.Structure):
         ("warm_start", C.c_int32),
         ("broadphase", C.c_int32),
         ("autotune", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("ls_groups", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

@@ -339,3 +339,95 @@ int eng_detect_bp(Engine* E, double filt) {
     E->launches++;
     return eng_pg_candidates(E, filt);
 }
+
+// ------------------------------------------------------------------ contact groups of the line search
+//
+// Two bodies belong to one group when their boxes swept over the listed
+// step x .. x + p, padded by half the candidate distance on every side,
+// overlap (transitively).  Bodies of different groups stay more than the
+// candidate distance apart for any pair of step fractions in [0, 1], so no
+// listed pair, barrier term or CCD bound couples them and each group can
+// take its own step length.  The union-find hooks the larger root under the
+// smaller with atomicCAS, so a group's root is its smallest body index.
+
+DV int grp_find(const int* parent, int x, int limit) {
+    for (int k = 0; k < limit; k++) {
+        int p = __ldcg(parent + x);
+        if (p == x) return x;
+        x = p;
+    }
+    return x;
+}
+
+__global__ void k_grp_init(int nb, int* parent) { GS_LOOP(b, nb) parent[b] = (int)b; }
+
+// one warp per body a: every later body b of the scene whose box overlaps
+__global__ void k_grp_union(int nb, const int* __restrict__ bscene, const int* __restrict__ sc_body_begin,
+                            const float4* __restrict__ blo, const float4* __restrict__ bhi, int* parent, Counters* cnt) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    for (int a = warp; a < nb; a += (gridDim.x * blockDim.x) >> 5) {
+        int end = sc_body_begin[bscene[a] + 1];
+        float4 al = blo[a], ah = bhi[a];
+        for (int b = a + 1 + lane; b < end; b += 32) {
+            if (!overlap(al, ah, blo[b], bhi[b])) continue;
+            // every failed CAS means a root was hooked, which happens at
+            // most nb - 1 times in total
+            int ra = a, rb = b;
+            bool ok = false;
+            for (int k = 0; k <= nb; k++) {
+                ra = grp_find(parent, ra, nb + 1); rb = grp_find(parent, rb, nb + 1);
+                if (ra == rb) { ok = true; break; }
+                if (ra < rb) { int t = ra; ra = rb; rb = t; }
+                int old = atomicCAS(parent + ra, ra, rb);
+                if (old == ra) { ok = true; break; }
+                ra = old;
+            }
+            if (!ok) atomicExch(&cnt->grp_fail, 1);
+        }
+    }
+}
+
+// root per body; a unit (a root body) joins the line search when its scene
+// is still iterating, every other slot is skipped
+__global__ void k_grp_finish(int nb, int* parent, const int* __restrict__ bscene, const int* __restrict__ done,
+                             int* udone) {
+    GS_LOOP(b, nb) {
+        int r = grp_find(parent, (int)b, nb + 1);
+        parent[b] = r;
+        udone[b] = (r != (int)b) || done[bscene[b]];
+    }
+}
+
+void eng_groups_free(Engine* E) {
+    void* ps[] = {E->grp, E->gscd, E->gsci, E->grp_lo, E->grp_hi};
+    for (void* p : ps) if (p) cudaFree(p);
+    E->grp = nullptr; E->gscd = nullptr; E->gsci = nullptr; E->grp_lo = nullptr; E->grp_hi = nullptr;
+}
+
+// groups of the step listed by the last eng_swept (positions E->x, step
+// E->pv); needs contiguous per-body vertex ranges
+int eng_groups(Engine* E, const int* done) {
+    if (!E->bd_ok) return E->fail(ABD_ERR_INVALID_ARG, "ls_groups needs contiguous per-body vertex ranges");
+    int nb = E->nb;
+    cudaStream_t s = E->stream;
+    if (!E->grp) {
+        if (cudaMalloc(&E->grp, sizeof(int) * nb) != cudaSuccess ||
+            cudaMalloc(&E->gscd, sizeof(double) * SD_COUNT * nb) != cudaSuccess ||
+            cudaMalloc(&E->gsci, sizeof(int) * SI_COUNT * nb) != cudaSuccess ||
+            cudaMalloc(&E->grp_lo, sizeof(float4) * nb) != cudaSuccess ||
+            cudaMalloc(&E->grp_hi, sizeof(float4) * nb) != cudaSuccess) {
+            eng_groups_free(E);
+            return E->fail(ABD_ERR_CUDA, "cudaMalloc contact groups");
+        }
+        CUDA_TRY(cudaMemsetAsync(E->gscd, 0, sizeof(double) * SD_COUNT * nb, s));
+        CUDA_TRY(cudaMemsetAsync(E->gsci, 0, sizeof(int) * SI_COUNT * nb, s));
+    }
+    double lim = E->P.cand_dist * (1.0 + 1e-6) + 1e-7;
+    float pad = (float)(0.5 * lim);
+    k_grp_init<<<grid_for(nb), 256, 0, s>>>(nb, E->grp);
+    k_body_boxes<<<grid_for(32L * nb), 256, 0, s>>>(nb, E->bd_vbeg, E->x, E->pv, pad, E->grp_lo, E->grp_hi);
+    k_grp_union<<<grid_for(32L * nb), 256, 0, s>>>(nb, E->bscene, E->sc_body_begin, E->grp_lo, E->grp_hi, E->grp, E->dcnt);
+    k_grp_finish<<<grid_for(nb), 256, 0, s>>>(nb, E->grp, E->bscene, done, E->gsci + SI_DONE * nb);
+    E->launches += 4;
+    return ABD_OK;
+}

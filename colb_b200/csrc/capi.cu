@@ -146,6 +146,7 @@ void eng_free(Engine* E) {
     eng_features_free(E);
     eng_mlp_free(E);
     eng_bp_free(E);
+    eng_groups_free(E);
     void* bd[] = {E->bd_vbeg, E->bd_ebeg, E->bd_tbeg};
     for (void* p : bd) if (p) cudaFree(p);
     grid_free(E->gee); grid_free(E->gpt);
@@ -208,8 +209,9 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     if (device < 0 || device >= ndev) { g_err = "abd_create: bad device index"; return ABD_ERR_INVALID_ARG; }
     const AbdParams& P = *params;
     if (!(P.dt > 0) || !(P.dhat > 0) || !(P.cand_dist >= P.dhat) || P.newton_max_iter <= 0 || P.lin_max_iter <= 0 ||
-        P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || P.linear_solver < 0 || P.linear_solver > 3 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1))) {
-        g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale)";
+        P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || P.linear_solver < 0 || P.linear_solver > 3 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1)) ||
+        P.ls_groups < 0 || P.ls_groups > 1) {
+        g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale, ls_groups)";
         return ABD_ERR_INVALID_ARG;
     }
     Engine* E = new (std::nothrow) Engine();
@@ -304,6 +306,10 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
         for (int e = 0; e < E->ne; e++) if (vbody[edges[2*e+1]] != eown[e]) ok = false;
         ranges(vbody, vb); ranges(eown, eb); ranges(town, tb);
         E->bd_ok = ok;
+        if (!ok && P.ls_groups) {
+            g_err = "abd_create: ls_groups needs every body to own a contiguous vertex range"; eng_free(E); delete E;
+            return ABD_ERR_INVALID_ARG;
+        }
         if (ok && ((rc = up(E->bd_vbeg, vb)) || (rc = up(E->bd_ebeg, eb)) || (rc = up(E->bd_tbeg, tb)))) {
             g_err = E->err; eng_free(E); delete E; return rc;
         }

@@ -35,8 +35,8 @@ __global__ void k_transform(int nv, const double* __restrict__ xbar, const int* 
     }
 }
 
-int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip);
-int eng_pg_energy(Engine* E, double* Eo, double* En, const int* skip);
+int eng_body_energy(Engine* E, const int* bunit, double* Eo, double* En, const int* skip);
+int eng_pg_energy(Engine* E, const int* bunit, double* Eo, double* En, const int* skip);
 int eng_pg_candidates(Engine* E, double filt);
 
 int eng_transform(Engine* E) {
@@ -481,14 +481,16 @@ __global__ void k_pt_energy(int nv, GridView GV, Geo G, const float4* __restrict
         warp_reduce_add(E, s, e, valid);
     }
 }
-__global__ void k_pg_energy(int nv, Geo G, const int* __restrict__ vscene, double dhat, int barrier, double sc,
-                            const int* done, double* E, double* En) {
+// planes come from the vertex's scene; the energy goes to the unit of its body
+__global__ void k_pg_energy(int nv, Geo G, const int* __restrict__ vscene, const int* __restrict__ bunit, double dhat,
+                            int barrier, double sc, const int* done, double* E, double* En) {
     for (long base = (long)blockIdx.x * blockDim.x; base < nv; base += (long)gridDim.x * blockDim.x) {
         long v = base + threadIdx.x;
         bool valid = v < nv;
         int s = valid ? vscene[v] : 0;
+        int u = valid ? bunit[G.vbody[v]] : 0;
         double e = 0, en = 0;
-        if (valid && !done[s]) {
+        if (valid && !done[u]) {
             double xh = dhat * dhat;
             double L = fmax(fabs(G.x[3*v]), fmax(fabs(G.x[3*v+1]), fabs(G.x[3*v+2])));
             for (int pl = G.sc_plane_begin[s]; pl < G.sc_plane_begin[s+1]; pl++) {
@@ -500,8 +502,8 @@ __global__ void k_pg_energy(int nv, Geo G, const int* __restrict__ vscene, doubl
                 en += contact_noise(sc, b0, b1, d * d, fmax(L, fabs(n[3])), 1.0) * DBL_EPSILON;
             }
         } else valid = false;
-        warp_reduce_add(E, s, e, valid);
-        if (En) warp_reduce_add(En, s, en, valid);
+        warp_reduce_add(E, u, e, valid);
+        if (En) warp_reduce_add(En, u, en, valid);
     }
 }
 
@@ -514,7 +516,7 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
     CUDA_TRY(cudaMemsetAsync(Eo, 0, sizeof(double) * E->ns, s));
     if ((rc = eng_transform(E))) return rc;
     const AbdParams& P = E->P;
-    if ((rc = eng_body_energy(E, Eo, nullptr, skip))) return rc;
+    if ((rc = eng_body_energy(E, E->bscene, Eo, nullptr, skip))) return rc;
     double sc = P.kappa * P.dt * P.dt;
     Geo G = geo(E);
     if (P.contact_ee && E->ne > 1) {
@@ -537,22 +539,22 @@ static int energy_impl(Engine* E, int slot, const int* skip) {
         phase_end(E, ph, E->nv * (32.0 + 4.0 + 24.0) + E->nt * (12.0 + 32.0 + 4.0 + 4.0) + g.H * 8.0);
         E->launches++;
     }
-    return eng_pg_energy(E, Eo, nullptr, skip);
+    return eng_pg_energy(E, E->bscene, Eo, nullptr, skip);
 }
 // En (may be null) accumulates the scale of the FP64 evaluation error
-int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip) {
+int eng_body_energy(Engine* E, const int* bunit, double* Eo, double* En, const int* skip) {
     const AbdParams& P = E->P;
     int tb = TUNE_THREADS[tune_begin(E, TK_BODY_ENERGY, 4, 2)];
-    k_body_energy<<<grid_for(E->nb, tb), tb, 0, E->stream>>>(E->nb, E->st, E->mass, E->J, E->bscene, P.dt, P.gravity[0],
+    k_body_energy<<<grid_for(E->nb, tb), tb, 0, E->stream>>>(E->nb, E->st, E->mass, E->J, bunit, P.dt, P.gravity[0],
                                                             P.gravity[1], P.gravity[2], P.k_ortho, skip, Eo, En);
     tune_end(E, TK_BODY_ENERGY);
     E->launches++;
     return ABD_OK;
 }
-int eng_pg_energy(Engine* E, double* Eo, double* En, const int* skip) {
+int eng_pg_energy(Engine* E, const int* bunit, double* Eo, double* En, const int* skip) {
     const AbdParams& P = E->P;
     if (E->npl > 0) {
-        k_pg_energy<<<grid_for(E->nv), 256, 0, E->stream>>>(E->nv, geo(E), E->vscene, P.dhat, P.barrier,
+        k_pg_energy<<<grid_for(E->nv), 256, 0, E->stream>>>(E->nv, geo(E), E->vscene, bunit, P.dhat, P.barrier,
                                                             P.kappa * P.dt * P.dt, skip, Eo, En);
         E->launches++;
     }

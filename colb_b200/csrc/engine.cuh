@@ -91,7 +91,7 @@ struct Counters {
     int n_ee, n_pt, n_pg, n_total;
     int overflow, nnzb, n_active, scenes_done;
     int krylov_active, ccd_capped, nan_flag, ls_pending;
-    int nkeys, pad0, pad1, pad2;
+    int nkeys, grp_fail, pad1, pad2;
     int n_sw, n_sw_ee, sw_overflow, pad3;
 };
 #define DETECT_COUNTER_BYTES (5 * sizeof(int))   // n_ee .. overflow
@@ -157,6 +157,13 @@ struct Engine {
     // per-scene scalars
     double* scd = nullptr;         // [NSCD][ns]
     int* sci = nullptr;            // [NSCI][ns]
+    // contact groups of the line search (ls_groups): group root body of
+    // each body, the per-group scalars in the per-scene layout with nb
+    // slots (a group's slot is its root body), and the swept body boxes
+    int* grp = nullptr;            // [nb]
+    double* gscd = nullptr;        // [NSCD][nb]
+    int* gsci = nullptr;           // [NSCI][nb]
+    float4* grp_lo = nullptr; float4* grp_hi = nullptr;   // [nb]
 
     // cub scratch
     void* cub_tmp = nullptr; size_t cub_bytes = 0;
@@ -212,7 +219,15 @@ enum {
     SD_COUNT
 };
 // per-scene int slots
-enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_STALL, SI_COUNT };
+enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_STALL, SI_GACT, SI_GSTALL, SI_COUNT };
+
+// The units the line search runs over: scenes (one step length per scene,
+// the reference's line search) or contact groups (ls_groups).  bunit maps a
+// body to its unit; d and i hold the unit scalars in the SD_* / SI_* layouts
+// with n slots each.
+struct LsUnits { int n; const int* bunit; double* d; int* i; };
+inline LsUnits scene_units(Engine* E) { return LsUnits{E->ns, E->bscene, E->scd, E->sci}; }
+inline LsUnits group_units(Engine* E) { return LsUnits{E->nb, E->grp, E->gscd, E->gsci}; }
 
 // launch helpers
 inline int grid_for(long n, int block = 256) {
@@ -268,8 +283,10 @@ int eng_sync_counters(Engine* E);
 int eng_grid_build(Engine* E, Grid& G);
 GridView eng_view(const Grid& G);
 int eng_swept(Engine* E, const double* dq, double sign, const int* done);
-int eng_ccd_list(Engine* E, const int* skip);
-int eng_energy_list(Engine* E, int slot, const int* skip);
+int eng_ccd_list(Engine* E, const LsUnits& U, const int* skip);
+int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip);
+int eng_groups(Engine* E, const int* done);   // contact groups of the listed step (after eng_swept)
+void eng_groups_free(Engine* E);
 int eng_detect_list(Engine* E);
 int eng_swept_bp(Engine* E, double lim);
 int eng_detect_bp(Engine* E, double filt);

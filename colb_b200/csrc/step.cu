@@ -22,10 +22,39 @@ __global__ void k_apply(int nb, const double* __restrict__ backup, const double*
         st[ST_STRIDE * b + ST_NXT + (i % 12)] = __fma_rn(-alpha[s], du[i], backup[i]);
     }
 }
-__global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, const double* toi, int ccd) {
+__global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, const double* toi, int ccd, int* stall) {
     GS_LOOP(s, ns) {
         acc[s] = done[s];
         alpha[s] = ccd ? fmin(1.0, toi[s]) : 1.0;
+        if (!done[s]) stall[s] = 0;
+    }
+}
+// contact groups -> scenes: the smallest step length and CCD bound of the
+// scene's groups (for the profile and the step statistics); the scene
+// stalls when every group that searched gave up below ABD_LS_STALL_ALPHA
+__global__ void k_grp_scene_init(int ns, const int* done, double* alpha, double* toi, int* gact, int* gstall) {
+    GS_LOOP(s, ns) {
+        if (done[s]) continue;
+        alpha[s] = 1.0; toi[s] = 1.0; gact[s] = 0; gstall[s] = 0;
+    }
+}
+__global__ void k_grp_to_scenes(int nb, const int* __restrict__ bscene, const int* __restrict__ udone,
+                                const double* __restrict__ ualpha, const double* __restrict__ utoi,
+                                const int* __restrict__ ustall, int ccd, double* alpha, double* toi, int* gact,
+                                int* gstall) {
+    GS_LOOP(u, nb) {
+        if (udone[u]) continue;
+        int s = bscene[u];
+        atomic_min_pos(alpha + s, ualpha[u]);
+        if (ccd) atomic_min_pos(toi + s, utoi[u]);
+        atomicAdd(gact + s, 1);
+        if (ustall[u]) atomicAdd(gstall + s, 1);
+    }
+}
+__global__ void k_grp_scene_stall(int ns, const int* done, const int* gact, const int* gstall, int* stall) {
+    GS_LOOP(s, ns) {
+        if (done[s]) continue;
+        stall[s] = gact[s] > 0 && gstall[s] == gact[s];
     }
 }
 // gauss_newton.py:107-113; an energy change within the FP64 evaluation
@@ -152,17 +181,17 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             // now + a ws, a = min(1, toi) halved until the energy is below
             // that of now (at most 7 halvings, else a = 0)
             if ((rc = eng_swept(E, E->ws, 1.0, done))) return rc;
-            if (P.ccd && (rc = eng_ccd_list(E, done))) return rc;
+            if (P.ccd && (rc = eng_ccd_list(E, scene_units(E), done))) return rc;
             k_ws_to_du<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->ws, E->mass, E->du);
             k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
-            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
+            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd, stall);
             E->launches += 3;
-            if ((rc = eng_energy_list(E, SD_E0, done))) return rc;
+            if ((rc = eng_energy_list(E, scene_units(E), SD_E0, done))) return rc;
             for (int trial = 0;; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
                 E->launches++;
                 if (trial == 8) break;
-                if ((rc = eng_energy_list(E, SD_E1, acc))) return rc;
+                if ((rc = eng_energy_list(E, scene_units(E), SD_E1, acc))) return rc;
                 k_ws_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, trial == 7, E->dcnt);
                 E->launches++;
                 if ((rc = eng_sync_counters(E))) return rc;
@@ -199,28 +228,52 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
                 phase_end(E, ph, E->nv * (24.0 + 24.0 + 4.0) + E->nb * 96.0 + E->ne * 8.0 + E->nt * 12.0 + E->n_sw * 24.0);
                 if (rc) return rc;
             }
+            // the line search runs per scene, or per contact group of the
+            // listed step (ls_groups): each unit has its own CCD bound,
+            // energies, step length and back-off
+            const bool groups = P.ls_groups && E->bd_ok;
+            // eng_groups allocates the group slots on first use: take the
+            // unit view only after it
+            if (groups && (rc = eng_groups(E, done))) return rc;
+            if (groups && !(E->grp && E->gscd && E->gsci)) return E->fail(ABD_ERR_CUDA, "contact groups not allocated");
+            LsUnits U = groups ? group_units(E) : scene_units(E);
+            const int* udone = U.i + SI_DONE * U.n;
+            int* uacc = U.i + SI_ACC * U.n;
+            int* ustall = U.i + SI_STALL * U.n;
+            double* ualpha = U.d + SD_ALPHA * U.n;
+            if (!groups) udone = done;
             if (P.ccd) {
-                int ph = phase_begin(E, PH_CCD); rc = eng_ccd_list(E, done); phase_end(E, ph, 0);
+                int ph = phase_begin(E, PH_CCD); rc = eng_ccd_list(E, U, udone); phase_end(E, ph, 0);
                 if (rc) return rc;
             }
             // gauss_newton.py:98-115 line search
-            { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E0, done); phase_end(E, ph, 0); if (rc) return rc; }
+            { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, U, SD_E0, udone); phase_end(E, ph, 0); if (rc) return rc; }
             k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
             E->launches++;
-            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd);
+            k_ls_init<<<grid_for(U.n), 256, 0, s>>>(U.n, udone, uacc, ualpha, U.d + SD_TOI * U.n, P.ccd, ustall);
             E->launches++;
             int ph_tr = phase_begin(E, PH_TRIALS);
             for (int trial = 0; trial < 64; trial++) {
-                k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, alpha, acc, E->bscene, E->st);
-                { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, SD_E1, acc); phase_end(E, ph, 0); if (rc) return rc; }
-                k_ls_decide<<<1, 256, 0, s>>>(ns, acc, alpha, E->scd + SD_E0 * ns, E->scd + SD_E1 * ns, E->scd + SD_E0N * ns,
-                                              E->scd + SD_E1N * ns, P.ls_min_alpha, stall, E->dcnt);
+                k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, ualpha, uacc, U.bunit, E->st);
+                { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, U, SD_E1, uacc); phase_end(E, ph, 0); if (rc) return rc; }
+                k_ls_decide<<<1, 256, 0, s>>>(U.n, uacc, ualpha, U.d + SD_E0 * U.n, U.d + SD_E1 * U.n, U.d + SD_E0N * U.n,
+                                              U.d + SD_E1N * U.n, P.ls_min_alpha, ustall, E->dcnt);
                 E->launches += 2;
                 st.ls_trials++;
                 if ((rc = eng_sync_counters(E))) return rc;
+                if (E->hcnt->grp_fail) return E->fail(ABD_ERR_CUDA, "contact groups: union-find did not settle");
                 if (E->hcnt->ls_pending == 0) break;
             }
             phase_end(E, ph_tr, 0);
+            if (groups) {
+                int* gact = E->sci + SI_GACT * ns; int* gstall = E->sci + SI_GSTALL * ns;
+                double* stoi = E->scd + SD_TOI * ns;
+                k_grp_scene_init<<<grid_for(ns), 256, 0, s>>>(ns, done, alpha, stoi, gact, gstall);
+                k_grp_to_scenes<<<grid_for(E->nb), 256, 0, s>>>(E->nb, E->bscene, udone, ualpha, U.d + SD_TOI * U.n, ustall,
+                                                                P.ccd, alpha, stoi, gact, gstall);
+                k_grp_scene_stall<<<grid_for(ns), 256, 0, s>>>(ns, done, gact, gstall, stall);
+                E->launches += 3;
+            }
             k_newton_book<<<1, 256, 0, s>>>(ns, done, iter, stall, E->scd + SD_GG * ns, alpha, prof_res, prof_alpha, mi,
                                             P.newton_tol, E->dcnt);
             E->launches++;

@@ -267,11 +267,13 @@ __global__ void k_ccd_list(int n, const int4* __restrict__ list, Geo G, const do
         if (accd(kind, xx, pp, s_ccd, 1.0, &t, capped)) atomic_min_pos(toi + s, t);
     }
 }
-__global__ void k_ccd_pg2(int nv, Geo G, const double* __restrict__ p, const int* __restrict__ vscene, double s_ccd,
-                          const int* skip, double* toi) {
+// planes come from the vertex's scene; the bound goes to the unit of its body
+__global__ void k_ccd_pg2(int nv, Geo G, const double* __restrict__ p, const int* __restrict__ vscene,
+                          const int* __restrict__ bunit, double s_ccd, const int* skip, double* toi) {
     GS_LOOP(v, nv) {
         int s = vscene[v];
-        if (skip[s]) continue;
+        int u = bunit[G.vbody[v]];
+        if (skip[u]) continue;
         double best = 1.0;
         for (int pl = G.sc_plane_begin[s]; pl < G.sc_plane_begin[s+1]; pl++) {
             const double* n = G.planes + 4*pl;
@@ -279,23 +281,24 @@ __global__ void k_ccd_pg2(int nv, Geo G, const double* __restrict__ p, const int
             double vn = n[0] * p[3*v] + n[1] * p[3*v+1] + n[2] * p[3*v+2];
             if (vn < 0) { double t = (1 - s_ccd) * d / (-vn); if (t < 0) t = 0; if (t < best) best = t; }
         }
-        if (best < 1.0) atomic_min_pos(toi + s, best);
+        if (best < 1.0) atomic_min_pos(toi + u, best);
     }
 }
 __global__ void k_fill1(double* a, int n, double v) { GS_LOOP(i, n) a[i] = v; }
 
-// per-scene largest conservative fraction of the listed displacement (E->pv)
-int eng_ccd_list(Engine* E, const int* skip) {
+// per-unit (scene or contact group) largest conservative fraction of the
+// listed displacement (E->pv) into U's SD_TOI slots
+int eng_ccd_list(Engine* E, const LsUnits& U, const int* skip) {
     cudaStream_t s = E->stream;
-    double* toi = E->scd + SD_TOI * E->ns;
-    k_fill1<<<grid_for(E->ns), 256, 0, s>>>(toi, E->ns, 1.0);
+    double* toi = U.d + SD_TOI * U.n;
+    k_fill1<<<grid_for(U.n), 256, 0, s>>>(toi, U.n, 1.0);
     int rc = eng_transform(E);
     if (rc) return rc;
     Geo G = eng_geo(E);
     if (E->n_sw > 0)
-        k_ccd_list<<<grid_for(E->n_sw, 64), 64, 0, s>>>(E->n_sw, E->sw, G, E->pv, E->bscene, skip, E->P.ccd_scale, toi,
+        k_ccd_list<<<grid_for(E->n_sw, 64), 64, 0, s>>>(E->n_sw, E->sw, G, E->pv, U.bunit, skip, E->P.ccd_scale, toi,
                                                         &E->dcnt->ccd_capped);
-    if (E->npl > 0) k_ccd_pg2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, G, E->pv, E->vscene, E->P.ccd_scale, skip, toi);
+    if (E->npl > 0) k_ccd_pg2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, G, E->pv, E->vscene, U.bunit, E->P.ccd_scale, skip, toi);
     E->launches += 1 + (E->n_sw > 0) + (E->npl > 0);
     return ABD_OK;
 }
@@ -335,32 +338,33 @@ __global__ void k_list_energy(int n, const int4* __restrict__ list, Geo G, const
     }
 }
 
-int eng_body_energy(Engine* E, double* Eo, double* En, const int* skip);
-int eng_pg_energy(Engine* E, double* Eo, double* En, const int* skip);
+int eng_body_energy(Engine* E, const int* bunit, double* Eo, double* En, const int* skip);
+int eng_pg_energy(Engine* E, const int* bunit, double* Eo, double* En, const int* skip);
 
-// energy per scene into scd[slot] and the scale of its FP64 evaluation
-// error into scd[noise slot] (SD_E0 -> SD_E0N, SD_E1 -> SD_E1N)
-int eng_energy_list(Engine* E, int slot, const int* skip) {
+// energy per unit (scene or contact group) into U's slot and the scale of
+// its FP64 evaluation error into the noise slot (SD_E0 -> SD_E0N,
+// SD_E1 -> SD_E1N)
+int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
-    double* Eo = E->scd + slot * E->ns;
-    double* En = E->scd + (slot == SD_E0 ? SD_E0N : SD_E1N) * E->ns;
-    CUDA_TRY(cudaMemsetAsync(Eo, 0, sizeof(double) * E->ns, s));
-    CUDA_TRY(cudaMemsetAsync(En, 0, sizeof(double) * E->ns, s));
+    double* Eo = U.d + slot * U.n;
+    double* En = U.d + (slot == SD_E0 ? SD_E0N : SD_E1N) * U.n;
+    CUDA_TRY(cudaMemsetAsync(Eo, 0, sizeof(double) * U.n, s));
+    CUDA_TRY(cudaMemsetAsync(En, 0, sizeof(double) * U.n, s));
     int rc = eng_transform(E);
     if (rc) return rc;
-    if ((rc = eng_body_energy(E, Eo, En, skip))) return rc;
+    if ((rc = eng_body_energy(E, U.bunit, Eo, En, skip))) return rc;
     if (E->n_sw > 0) {
         int ph = phase_begin(E, PH_ELIST);
         int tb = TUNE_THREADS[tune_begin(E, TK_LIST_ENERGY, 4, 1)];
-        k_list_energy<<<grid_for(E->n_sw, tb), tb, 0, s>>>(E->n_sw, E->sw, eng_geo(E), E->bscene, skip, P.ee_f32, P.dhat,
+        k_list_energy<<<grid_for(E->n_sw, tb), tb, 0, s>>>(E->n_sw, E->sw, eng_geo(E), U.bunit, skip, P.ee_f32, P.dhat,
                                                            P.barrier, P.kappa * P.dt * P.dt, Eo, En);
         tune_end(E, TK_LIST_ENERGY);
         // per listed pair: the entry, its 2-4 vertex ids and positions
         phase_end(E, ph, E->n_sw * (16.0 + 16.0 + 4 * 24.0));
         E->launches++;
     }
-    return eng_pg_energy(E, Eo, En, skip);
+    return eng_pg_energy(E, U.bunit, Eo, En, skip);
 }
 
 // ------------------------------------------------------------------ detection from the list

@@ -48,6 +48,7 @@ REFERENCE = dict(
     pinned_diag=100.0,
     warm_start=0,
     autotune=1,
+    ls_groups=0,
 )
 
 CONFIG = dict(
@@ -76,6 +77,7 @@ CONFIG = dict(
     pinned_diag=100.0,
     warm_start=0,
     autotune=1,
+    ls_groups=0,
 )
 
 

@@ -110,7 +110,14 @@ typedef struct AbdParams {
     int32_t autotune;       /* 1: time the launch-shape candidates of the tunable kernels during
                                the first Newton iterations of the handle and keep the fastest
                                (abd_get_autotune); 0: fixed launch shapes */
-    int32_t reserved[5];
+    int32_t ls_groups;      /* 0: one step length per scene, as gauss_newton.py:98-115 does for
+                               its one scene; 1: one step length per contact group, the
+                               connected components of the bodies whose swept, padded boxes
+                               over the Newton step overlap (no contact can form between
+                               groups along the step, so the energy is a sum of independent
+                               group energies and each group takes its own CCD bound and
+                               back-off).  Convergence stays per scene. */
+    int32_t reserved[4];
 } AbdParams;
 
 /* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */

@@ -1261,6 +1261,209 @@ static void prof_push(OScene* S, double res, double alpha) {
     S->prof_res[S->prof_n] = res; S->prof_alpha[S->prof_n] = alpha; S->prof_n++;
 }
 
+/* ------------------------------------------------------------------ */
+/* Contact groups of the line search (AbdParams.ls_groups; no reference */
+/* counterpart).  Bodies whose boxes swept over x .. x + p, rounded      */
+/* outward to float and padded by half the candidate distance, overlap  */
+/* are joined (transitively); a group is named by its smallest body.    */
+/* ------------------------------------------------------------------ */
+static float f_rd(double d) { float f = (float)d; if ((double)f > d) f = nextafterf(f, -INFINITY); return f; }
+static float f_ru(double d) { float f = (float)d; if ((double)f < d) f = nextafterf(f, INFINITY); return f; }
+/* float a - b rounded down / a + b rounded up (the exact result is a double
+ * when the exponents of a and b are within 28 of each other) */
+static float fsub_rd(float a, float b) { return f_rd((double)a - (double)b); }
+static float fadd_ru(float a, float b) { return f_ru((double)a + (double)b); }
+static int grp_root(int* parent, int x) {
+    int r = x;
+    while (parent[r] != r) r = parent[r];
+    while (parent[x] != r) { int n = parent[x]; parent[x] = r; x = n; }
+    return r;
+}
+/* gid[b] = smallest body index of b's group */
+static void contact_groups(const OracleWorld* w, const OScene* S, const double* x, const double* p, int* gid) {
+    int nb = S->nb;
+    double lim = w->P.cand_dist * (1.0 + 1e-6) + 1e-7;
+    float pad = (float)(0.5 * lim);
+    float* box = (float*)xalloc(sizeof(float) * 6 * nb);
+    for (int b = 0; b < nb; b++) for (int k = 0; k < 3; k++) { box[6*b+k] = 3e38f; box[6*b+3+k] = -3e38f; }
+    for (int v = 0; v < S->nv; v++) {
+        int b = S->vbody[v];
+        for (int k = 0; k < 3; k++) {
+            double a = x[3*v+k], e = a + p[3*v+k];
+            float lo = fsub_rd(f_rd(fmin(a, e)), pad), hi = fadd_ru(f_ru(fmax(a, e)), pad);
+            box[6*b+k] = fminf(box[6*b+k], lo); box[6*b+3+k] = fmaxf(box[6*b+3+k], hi);
+        }
+    }
+    for (int b = 0; b < nb; b++) gid[b] = b;
+    for (int a = 0; a < nb; a++) {
+        const float* A = box + 6*a;
+        for (int b = a + 1; b < nb; b++) {
+            const float* B = box + 6*b;
+            if (A[0] > B[3] || A[3] < B[0] || A[1] > B[4] || A[4] < B[1] || A[2] > B[5] || A[5] < B[2]) continue;
+            int ra = grp_root(gid, a), rb = grp_root(gid, b);
+            if (ra == rb) continue;
+            if (ra < rb) gid[rb] = ra; else gid[ra] = rb;
+        }
+    }
+    for (int b = 0; b < nb; b++) gid[b] = grp_root(gid, b);
+    free(box);
+}
+/* energy and its FP64 error scale per group (slot = group root) */
+static void group_energy(const OracleWorld* w, OScene* S, const double* st, const int* gid, double* e, double* noise) {
+    int nb = S->nb;
+    for (int b = 0; b < nb; b++) { e[b] = 0; noise[b] = 0; }
+    for (int b = 0; b < nb; b++) { double n_; e[gid[b]] += body_energy(w, S, st, b, &n_); noise[gid[b]] += n_; }
+    transform(S, st, S->x);
+    detect(w, S, S->x, w->P.cand_dist);
+    double* ec = (double*)xalloc(sizeof(double) * 2 * (S->nc + 1));
+    #pragma omp parallel for num_threads(g_threads) schedule(dynamic, 64)
+    for (int c = 0; c < S->nc; c++) { CEval ce; eval_contact(w, S, S->x, &S->cand[c], 0, &ce); ec[2*c] = ce.e; ec[2*c+1] = ce.noise; }
+    for (int c = 0; c < S->nc; c++) {
+        const Cand* C = &S->cand[c];
+        int v0 = C->kind == ABD_CONTACT_EE ? S->edges[2*C->a] : C->a;
+        int g = gid[S->vbody[v0]];
+        e[g] += ec[2*c]; noise[g] += ec[2*c+1];
+    }
+    free(ec);
+}
+/* CCD bound per group over x -> x + p */
+typedef struct { const OracleWorld* w; const OScene* S; const double* x; const double* p; const int* gid; } GCcdCtx;
+/* a hit is kept as (group, the bits of t) in the sweep's per-thread list */
+static void gccd_pair(GCcdCtx* d, CandVec* out, int kind, const int v[4]) {
+    const AbdParams* P = &d->w->P;
+    double x[12], p[12];
+    for (int k = 0; k < 4; k++) { memcpy(x + 3*k, d->x + 3*v[k], 24); memcpy(p + 3*k, d->p + 3*v[k], 24); }
+    double t;
+    if (oracle_accd(kind, x, p, P->ccd_scale, 1.0, &t)) {
+        int bits[2]; memcpy(bits, &t, sizeof t);
+        cv_push(out, d->gid[d->S->vbody[v[0]]], bits[0], bits[1]);
+    }
+}
+static void gccd_ee_cb(void* c, CandVec* out, int i, int j) {
+    GCcdCtx* d = (GCcdCtx*)c; const OScene* S = d->S; const AbdParams* P = &d->w->P;
+    const int* ea = S->edges + 2*i; const int* eb = S->edges + 2*j;
+    if (ea[0] == eb[0] || ea[0] == eb[1] || ea[1] == eb[0] || ea[1] == eb[1]) return;
+    if (!P->self_contact && S->vbody[ea[0]] == S->vbody[eb[0]]) return;
+    int v[4] = {ea[0], ea[1], eb[0], eb[1]};
+    gccd_pair(d, out, 0, v);
+}
+static void gccd_pt_cb(void* c, CandVec* out, int pi, int ti) {
+    GCcdCtx* d = (GCcdCtx*)c; const OScene* S = d->S; const AbdParams* P = &d->w->P;
+    const int* tr = S->tris + 3*ti;
+    if (pi == tr[0] || pi == tr[1] || pi == tr[2]) return;
+    if (!P->self_contact && S->vbody[pi] == S->vbody[tr[0]]) return;
+    int v[4] = {pi, tr[0], tr[1], tr[2]};
+    gccd_pair(d, out, 1, v);
+}
+static void group_ccd(const OracleWorld* w, const OScene* S, const double* x, const double* p, const int* gid, double* toi) {
+    const AbdParams* P = &w->P;
+    for (int b = 0; b < S->nb; b++) toi[b] = 1.0;
+    GCcdCtx ctx = {w, S, x, p, gid};
+    CandVec hits = {0};
+    if (P->contact_ee && S->ne > 1) {
+        Box* bx = (Box*)xalloc(sizeof(Box) * S->ne);
+        for (int e = 0; e < S->ne; e++) {
+            int a = S->edges[2*e], b = S->edges[2*e+1];
+            for (int k = 0; k < 3; k++) {
+                double v0 = x[3*a+k], v1 = x[3*b+k], v2 = x[3*a+k] + p[3*a+k], v3 = x[3*b+k] + p[3*b+k];
+                bx[e].lo[k] = fmin(fmin(v0, v1), fmin(v2, v3)) - 1e-9; bx[e].hi[k] = fmax(fmax(v0, v1), fmax(v2, v3)) + 1e-9;
+            }
+            bx[e].id = e; bx[e].set = 0;
+        }
+        sweep(bx, S->ne, 0, gccd_ee_cb, &ctx, &hits);
+        free(bx);
+    }
+    if (P->contact_pt && S->nt > 0) {
+        Box* bx = (Box*)xalloc(sizeof(Box) * (S->nv + S->nt));
+        for (int v = 0; v < S->nv; v++) {
+            for (int k = 0; k < 3; k++) {
+                double a = x[3*v+k], b = a + p[3*v+k];
+                bx[v].lo[k] = fmin(a, b) - 1e-9; bx[v].hi[k] = fmax(a, b) + 1e-9;
+            }
+            bx[v].id = v; bx[v].set = 0;
+        }
+        for (int t = 0; t < S->nt; t++) {
+            Box* B = &bx[S->nv + t];
+            for (int k = 0; k < 3; k++) {
+                double lo = 1e300, hi = -1e300;
+                for (int q = 0; q < 3; q++) { int v = S->tris[3*t+q]; double a = x[3*v+k], b = a + p[3*v+k]; lo = fmin(lo, fmin(a, b)); hi = fmax(hi, fmax(a, b)); }
+                B->lo[k] = lo - 1e-9; B->hi[k] = hi + 1e-9;
+            }
+            B->id = t; B->set = 1;
+        }
+        sweep(bx, S->nv + S->nt, 1, gccd_pt_cb, &ctx, &hits);
+        free(bx);
+    }
+    for (int k = 0; k < hits.n; k++) {
+        double t; int bits[2] = {hits.v[k].a, hits.v[k].b}; memcpy(&t, bits, sizeof t);
+        if (t < toi[hits.v[k].kind]) toi[hits.v[k].kind] = t;
+    }
+    free(hits.v);
+    for (int pl = 0; pl < S->np; pl++) {
+        const double* n = S->planes + 4*pl;
+        for (int v = 0; v < S->nv; v++) {
+            double d = dot3(n, x + 3*v) - n[3], vn = dot3(n, p + 3*v);
+            if (vn < 0) {
+                double t = (1 - P->ccd_scale) * d / (-vn);
+                int g = gid[S->vbody[v]];
+                if (t < toi[g]) toi[g] = t < 0 ? 0 : t;
+            }
+        }
+    }
+}
+/* the line search with one step length per group: every group backs off
+ * on its own energy (gauss_newton.py:98-115 per group); returns the
+ * smallest accepted step, *stalled when every group gave up below
+ * ABD_LS_STALL_ALPHA, *min_toi the smallest CCD bound */
+static double group_line_search(const OracleWorld* w, OScene* S, const double* backup, const double* du, double* pv,
+                                int* stalled, double* min_toi, int* trials) {
+    const AbdParams* P = &w->P;
+    int nb = S->nb;
+    int* gid = (int*)xalloc(sizeof(int) * nb);
+    double* d = (double*)xalloc(sizeof(double) * 6 * nb);
+    double *E0 = d, *N0 = d + nb, *E1 = d + 2*nb, *N1 = d + 3*nb, *al = d + 4*nb, *toi = d + 5*nb;
+    int* acc = (int*)xalloc(sizeof(int) * 2 * nb);
+    int* stl = acc + nb;
+    transform(S, S->st, S->x);
+    vertex_disp(S, du, -1.0, pv);
+    contact_groups(w, S, S->x, pv, gid);
+    group_energy(w, S, S->st, gid, E0, N0);
+    if (P->ccd) group_ccd(w, S, S->x, pv, gid, toi);
+    *min_toi = 1.0;
+    for (int g = 0; g < nb; g++) {
+        acc[g] = gid[g] != g; stl[g] = 0;
+        al[g] = P->ccd ? fmin(1.0, toi[g]) : 1.0;
+        if (!acc[g] && P->ccd && toi[g] < *min_toi) *min_toi = toi[g];
+    }
+    for (;;) {
+        for (int b = 0; b < nb; b++) {
+            int g = gid[b];
+            if (acc[g]) continue;
+            double* nx = S->st + 48*b + ST_NXT; const double* bk = backup + 48*b + ST_NXT;
+            for (int k = 0; k < 12; k++) nx[k] = fma(-al[g], du[12*b + k], bk[k]);
+        }
+        group_energy(w, S, S->st, gid, E1, N1);
+        (*trials)++;
+        int pending = 0;
+        for (int g = 0; g < nb; g++) {
+            if (acc[g]) continue;
+            if (E1[g] < E0[g] || E1[g] - E0[g] <= N0[g] + N1[g]) acc[g] = 1;
+            else if (al[g] * 0.5 < P->ls_min_alpha) { acc[g] = 1; stl[g] = al[g] < ABD_LS_STALL_ALPHA; }
+            else { al[g] *= 0.5; pending++; }
+        }
+        if (!pending) break;
+    }
+    double amin = 1.0; int nact = 0, nst = 0;
+    for (int g = 0; g < nb; g++) {
+        if (gid[g] != g) continue;
+        nact++; nst += stl[g];
+        if (al[g] < amin) amin = al[g];
+    }
+    *stalled = nact > 0 && nst == nact;
+    free(gid); free(d); free(acc);
+    return amin;
+}
+
 static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
     const AbdParams* P = &w->P;
     int nb = S->nb;
@@ -1306,6 +1509,17 @@ static void scene_step(const OracleWorld* w, OScene* S, AbdStepStats* st) {
         free(as.g); bsr_free(&as.A);
         /* line search */
         memcpy(backup, S->st, sizeof(double) * 48 * nb);
+        if (P->ls_groups) {
+            int stalled = 0, trials = 0;
+            double mt = 1.0;
+            double alpha = group_line_search(w, S, backup, du, pv, &stalled, &mt, &trials);
+            st->ls_trials += trials;
+            if (mt < st->min_toi) st->min_toi = mt;
+            it++;
+            prof_push(S, res, alpha);
+            if (res < P->newton_tol || it >= P->newton_max_iter || stalled) break;
+            continue;
+        }
         double N0, N1;
         double E0 = scene_energy(w, S, S->st, &N0);
         double alpha = 1.0;
