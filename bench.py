@@ -221,6 +221,9 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     scenes, p, cfg = make_workload(args.workload, rank, args.precision, world=world)
+    if args.ls_graph is not None:
+        p.ls_graph = args.ls_graph
+    cfg = dict(cfg, line_search="one CUDA graph per Newton iteration" if p.ls_graph else "host loop per trial")
     if args.ls_groups:
         p.ls_groups = 1
         cfg = dict(cfg, line_search="one step length per contact group")
@@ -241,7 +244,7 @@ def run_ours(args, rank, world):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    gpu_ms, launches, iters, unconv, lin = 0.0, 0, 0, 0, 0
+    gpu_ms, launches, iters, unconv, lin, graphs = 0.0, 0, 0, 0, 0, 0
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
             flush_l2(flush)
@@ -252,6 +255,7 @@ def run_ours(args, rank, world):
             iters += st.newton_iters
             unconv += st.unconverged
             lin += st.lin_iters
+            graphs += st.ls_graph_launches
     torch.cuda.synchronize()
     t = torch.tensor([gpu_ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -267,7 +271,8 @@ def run_ours(args, rank, world):
     nb = int(nbt.item()) if world > 1 else nb
     if args.profile:
         return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
-                    lin=lin, e2e_s=float("nan"), clocks=clk.summary(), phases=None, n_timing=0, bytes_state=48 * 8 * eng.nb)
+                    lin=lin, e2e_s=float("nan"), clocks=clk.summary(), phases=None, n_timing=0, bytes_state=48 * 8 * eng.nb,
+                    graphs=graphs)
     # ---- e2e through the public API with host buffers: H2D of the state,
     # one step, D2H of the state every step
     host_state = eng.get_state()
@@ -295,7 +300,7 @@ def run_ours(args, rank, world):
     eng.set_timing(False, True)
     return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
                 lin=lin, e2e_s=float(e2e_t.item()), clocks=clk.summary(), phases=phases, n_timing=n_timing,
-                bytes_state=48 * 8 * eng.nb)
+                bytes_state=48 * 8 * eng.nb, graphs=graphs)
 
 
 def run_forms(args, scenes, p, dev=0):
@@ -353,6 +358,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="net16", choices=["net16", "net16c", "chain", "cubes", "batch", "pile"])
     ap.add_argument("--ls-groups", type=int, default=0, choices=[0, 1], help="1: one step length per contact group")
+    ap.add_argument("--ls-graph", type=int, default=None, choices=[0, 1],
+                    help="1: line search as one CUDA graph per Newton iteration, 0: host loop (default: the workload's)")
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed FP32/FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warm-start", type=int, default=0, choices=[0, 2, 3], help="0 plain, 2 inertial, 3 learned network")
@@ -420,6 +427,7 @@ def main():
         "krylov_iters_per_step": r["lin"] / args.steps,
         "unconverged_steps": r["unconv"],
         "gpu_launches": r["launches"],
+        "ls_graph_launches": r["graphs"],
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": r["bytes_state"],
                 "d2h_bytes_per_step": r["bytes_state"]},
         "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -56,7 +56,8 @@ class AbdParams(C.Structure):
         ("broadphase", C.c_int32),
         ("autotune", C.c_int32),
         ("ls_groups", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("ls_graph", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -96,7 +97,7 @@ class AbdStepStats(C.Structure):
         ("comp_small", C.c_int32),
         ("comp_large", C.c_int32),
         ("krylov_fallbacks", C.c_int32),
-        ("reserved", C.c_int32 * 1),
+        ("ls_graph_launches", C.c_int32),
     ]
 
     def as_dict(self):

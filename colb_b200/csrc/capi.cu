@@ -147,6 +147,7 @@ void eng_free(Engine* E) {
     eng_mlp_free(E);
     eng_bp_free(E);
     eng_groups_free(E);
+    eng_lsgraph_free(E);
     void* bd[] = {E->bd_vbeg, E->bd_ebeg, E->bd_tbeg};
     for (void* p : bd) if (p) cudaFree(p);
     grid_free(E->gee); grid_free(E->gpt);
@@ -210,8 +211,8 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     const AbdParams& P = *params;
     if (!(P.dt > 0) || !(P.dhat > 0) || !(P.cand_dist >= P.dhat) || P.newton_max_iter <= 0 || P.lin_max_iter <= 0 ||
         P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || P.linear_solver < 0 || P.linear_solver > 3 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1)) ||
-        P.ls_groups < 0 || P.ls_groups > 1) {
-        g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale, ls_groups)";
+        P.ls_groups < 0 || P.ls_groups > 1 || P.ls_graph < 0 || P.ls_graph > 1) {
+        g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale, ls_groups, ls_graph)";
         return ABD_ERR_INVALID_ARG;
     }
     Engine* E = new (std::nothrow) Engine();
@@ -566,6 +567,7 @@ int tune_begin(Engine* E, int k, int ncand, int dflt) {
     Engine::Tuner& t = E->tune[k];
     if (!E->P.autotune) return dflt;
     if (t.chosen >= 0) return t.chosen;
+    if (E->capturing) return dflt;      // no timing inside a captured graph
     if (!t.a) { cudaEventCreate(&t.a); cudaEventCreate(&t.b); }
     if (t.running >= 0) {
         float ms = 0;
@@ -591,6 +593,7 @@ int tune_begin(Engine* E, int k, int ncand, int dflt) {
 }
 void tune_end(Engine* E, int k) {
     Engine::Tuner& t = E->tune[k];
+    if (E->capturing) return;
     if (t.running >= 0) cudaEventRecord(t.b, E->stream);
 }
 

@@ -91,7 +91,7 @@ struct Counters {
     int n_ee, n_pt, n_pg, n_total;
     int overflow, nnzb, n_active, scenes_done;
     int krylov_active, ccd_capped, nan_flag, ls_pending;
-    int nkeys, grp_fail, pad1, pad2;
+    int nkeys, grp_fail, ls_trials, ls_nsw;   // ls_*: trial count and list length of a graph line search
     int n_sw, n_sw_ee, sw_overflow, pad3;
 };
 #define DETECT_COUNTER_BYTES (5 * sizeof(int))   // n_ee .. overflow
@@ -164,6 +164,8 @@ struct Engine {
     double* gscd = nullptr;        // [NSCD][nb]
     int* gsci = nullptr;           // [NSCI][nb]
     float4* grp_lo = nullptr; float4* grp_hi = nullptr;   // [nb]
+    void* ls_graph_state = nullptr;   // line-search graphs (ls_graph, step.cu)
+    bool capturing = false;           // a graph body is being captured: the autotuner only reports its shape
 
     // cub scratch
     void* cub_tmp = nullptr; size_t cub_bytes = 0;
@@ -284,7 +286,10 @@ int eng_grid_build(Engine* E, Grid& G);
 GridView eng_view(const Grid& G);
 int eng_swept(Engine* E, const double* dq, double sign, const int* done);
 int eng_ccd_list(Engine* E, const LsUnits& U, const int* skip);
-int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip);
+// dev_count: the listed-pair kernel reads the list length from
+// dcnt->ls_nsw and runs a fixed grid (for a graph that outlives one list)
+int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip, bool dev_count = false);
+void eng_lsgraph_free(Engine* E);
 int eng_groups(Engine* E, const int* done);   // contact groups of the listed step (after eng_swept)
 void eng_groups_free(Engine* E);
 int eng_detect_list(Engine* E);

@@ -59,8 +59,9 @@ __global__ void k_grp_scene_stall(int ns, const int* done, const int* gact, cons
 }
 // gauss_newton.py:107-113; an energy change within the FP64 evaluation
 // error of the two energies (N0 + N1) is no increase
-__global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, const double* N0,
-                            const double* N1, double min_alpha, int* stall, Counters* cnt) {
+// one block: returns (to thread 0) the number of units still searching
+DV int ls_decide_block(int ns, int* acc, double* alpha, const double* E0, const double* E1, const double* N0,
+                       const double* N1, double min_alpha, int* stall) {
     __shared__ int pending;
     if (threadIdx.x == 0) pending = 0;
     __syncthreads();
@@ -71,7 +72,115 @@ __global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, c
         else { alpha[s] *= 0.5; atomicAdd(&pending, 1); }
     }
     __syncthreads();
+    return pending;
+}
+__global__ void k_ls_decide(int ns, int* acc, double* alpha, const double* E0, const double* E1, const double* N0,
+                            const double* N1, double min_alpha, int* stall, Counters* cnt) {
+    int pending = ls_decide_block(ns, acc, alpha, E0, E1, N0, N1, min_alpha, stall);
     if (threadIdx.x == 0) cnt->ls_pending = pending;
+}
+// the same decision inside the line-search graph: counts the trial and
+// keeps the graph's while-node running while units are pending, for at most
+// LS_MAX_TRIALS trials (the host loop's cap)
+constexpr int LS_MAX_TRIALS = 64;
+__global__ void k_ls_decide_graph(int ns, int* acc, double* alpha, const double* E0, const double* E1, const double* N0,
+                                  const double* N1, double min_alpha, int* stall, Counters* cnt,
+                                  cudaGraphConditionalHandle loop) {
+    int pending = ls_decide_block(ns, acc, alpha, E0, E1, N0, N1, min_alpha, stall);
+    if (threadIdx.x == 0) {
+        cnt->ls_pending = pending;
+        int t = cnt->ls_trials + 1;
+        cnt->ls_trials = t;
+        cudaGraphSetConditional(loop, (pending > 0 && t < LS_MAX_TRIALS) ? 1u : 0u);
+    }
+}
+__global__ void k_ls_graph_prep(Counters* cnt, int n_sw) { cnt->ls_trials = 0; cnt->ls_nsw = n_sw; }
+
+// Line-search graphs (ls_graph): one per unit kind (scenes, contact
+// groups), each a while-node whose body is one trial: apply the step
+// length, the energies of the listed step, the decision.  Every pointer in
+// the body is fixed for the handle except the swept list, which can be
+// reallocated when it grows: the graph is rebuilt then.
+struct LsGraph {
+    cudaGraph_t g = nullptr; cudaGraphExec_t x = nullptr;
+    const void* sw = nullptr;       // swept list the body was captured with
+    int shapes[2] = {-2, -2};       // autotuner choice (list, body energy) it was captured with
+    int body_launches = 0;          // kernels per trial
+};
+struct LsGraphState { LsGraph gr[2]; bool failed = false; };
+void eng_lsgraph_free(Engine* E) {
+    auto* S = reinterpret_cast<LsGraphState*>(E->ls_graph_state);
+    if (!S) return;
+    for (auto& g : S->gr) { if (g.x) cudaGraphExecDestroy(g.x); if (g.g) cudaGraphDestroy(g.g); }
+    delete S;
+    E->ls_graph_state = nullptr;
+}
+static int ls_graph_build(Engine* E, LsGraph& G, const LsUnits& U, const int* uacc, double* ualpha, int* ustall) {
+    cudaStream_t s = E->stream;
+    if (G.x) { cudaGraphExecDestroy(G.x); G.x = nullptr; }
+    if (G.g) { cudaGraphDestroy(G.g); G.g = nullptr; }
+    CUDA_TRY(cudaGraphCreate(&G.g, 0));
+    cudaGraphConditionalHandle h;
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&h, G.g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CUDA_TRY(cudaGraphAddNode(&node, G.g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const int l0 = E->launches;
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const AbdParams& P = E->P;
+    E->capturing = true;
+    k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, ualpha, uacc, U.bunit, E->st);
+    int rc = eng_energy_list(E, U, SD_E1, uacc, true);
+    k_ls_decide_graph<<<1, 256, 0, s>>>(U.n, const_cast<int*>(uacc), ualpha, U.d + SD_E0 * U.n, U.d + SD_E1 * U.n,
+                                        U.d + SD_E0N * U.n, U.d + SD_E1N * U.n, P.ls_min_alpha, ustall, E->dcnt, h);
+    E->capturing = false;
+    cudaGraph_t captured = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(s, &captured);
+    G.body_launches = E->launches - l0 + 2;
+    E->launches = l0;
+    if (rc) return rc;
+    CUDA_TRY(ce);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaGraphInstantiate(&G.x, G.g, 0));
+    G.sw = E->sw;
+    G.shapes[0] = E->tune[TK_LIST_ENERGY].chosen; G.shapes[1] = E->tune[TK_BODY_ENERGY].chosen;
+    return ABD_OK;
+}
+// the line search of one Newton iteration as one graph launch; returns
+// ABD_OK with *ran = 0 when the graph cannot be used (the caller then runs
+// the host loop)
+static int ls_graph_run(Engine* E, bool groups, const LsUnits& U, const int* uacc, double* ualpha, int* ustall,
+                        int* trials, int* ran) {
+    *ran = 0;
+    if (!E->ls_graph_state) E->ls_graph_state = new LsGraphState();
+    auto* S = reinterpret_cast<LsGraphState*>(E->ls_graph_state);
+    if (S->failed || E->timing) return ABD_OK;
+    LsGraph& G = S->gr[groups ? 1 : 0];
+    // captured again when the swept list moved or the autotuner settled
+    // on a launch shape after the capture
+    if (!G.x || G.sw != E->sw || G.shapes[0] != E->tune[TK_LIST_ENERGY].chosen ||
+        G.shapes[1] != E->tune[TK_BODY_ENERGY].chosen) {
+        if (ls_graph_build(E, G, U, uacc, ualpha, ustall)) {
+            // graphs unavailable: keep the host loop for this handle
+            S->failed = true;
+            cudaGetLastError();
+            E->err.clear();
+            return ABD_OK;
+        }
+    }
+    k_ls_graph_prep<<<1, 1, 0, E->stream>>>(E->dcnt, E->n_sw);
+    CUDA_TRY(cudaGraphLaunch(G.x, E->stream));
+    int rc = eng_sync_counters(E);
+    if (rc) return rc;
+    *trials = E->hcnt->ls_trials;
+    E->launches += 1 + G.body_launches * E->hcnt->ls_trials;
+    *ran = 1;
+    return ABD_OK;
 }
 // abd.py:693-699 bookkeeping: record (residual, alpha), stop on tol or cap
 __global__ void k_newton_book(int ns, int* done, int* iter, const int* stall, const double* gg, const double* alpha,
@@ -253,7 +362,17 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             k_ls_init<<<grid_for(U.n), 256, 0, s>>>(U.n, udone, uacc, ualpha, U.d + SD_TOI * U.n, P.ccd, ustall);
             E->launches++;
             int ph_tr = phase_begin(E, PH_TRIALS);
-            for (int trial = 0; trial < 64; trial++) {
+            int graph_ran = 0;
+            if (P.ls_graph) {
+                int nt = 0;
+                if ((rc = ls_graph_run(E, groups, U, uacc, ualpha, ustall, &nt, &graph_ran))) return rc;
+                if (graph_ran) {
+                    st.ls_trials += nt;
+                    st.ls_graph_launches++;
+                    if (E->hcnt->grp_fail) return E->fail(ABD_ERR_CUDA, "contact groups: union-find did not settle");
+                }
+            }
+            for (int trial = 0; trial < LS_MAX_TRIALS && !graph_ran; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, ualpha, uacc, U.bunit, E->st);
                 { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, U, SD_E1, uacc); phase_end(E, ph, 0); if (rc) return rc; }
                 k_ls_decide<<<1, 256, 0, s>>>(U.n, uacc, ualpha, U.d + SD_E0 * U.n, U.d + SD_E1 * U.n, U.d + SD_E0N * U.n,

@@ -304,9 +304,10 @@ int eng_ccd_list(Engine* E, const LsUnits& U, const int* skip) {
 }
 
 // ------------------------------------------------------------------ energy over the list
-__global__ void k_list_energy(int n, const int4* __restrict__ list, Geo G, const int* __restrict__ bscene,
-                              const int* __restrict__ skip, int f32, double dhat, int barrier, double sc, double* Eo,
-                              double* En) {
+__global__ void k_list_energy(int n, const int* __restrict__ n_dev, const int4* __restrict__ list, Geo G,
+                              const int* __restrict__ bscene, const int* __restrict__ skip, int f32, double dhat,
+                              int barrier, double sc, double* Eo, double* En) {
+    if (n_dev) n = *n_dev;
     for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
         long c = base + threadIdx.x;
         bool valid = c < n;
@@ -344,7 +345,7 @@ int eng_pg_energy(Engine* E, const int* bunit, double* Eo, double* En, const int
 // energy per unit (scene or contact group) into U's slot and the scale of
 // its FP64 evaluation error into the noise slot (SD_E0 -> SD_E0N,
 // SD_E1 -> SD_E1N)
-int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip) {
+int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip, bool dev_count) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
     double* Eo = U.d + slot * U.n;
@@ -354,11 +355,12 @@ int eng_energy_list(Engine* E, const LsUnits& U, int slot, const int* skip) {
     int rc = eng_transform(E);
     if (rc) return rc;
     if ((rc = eng_body_energy(E, U.bunit, Eo, En, skip))) return rc;
-    if (E->n_sw > 0) {
+    if (E->n_sw > 0 || dev_count) {
         int ph = phase_begin(E, PH_ELIST);
         int tb = TUNE_THREADS[tune_begin(E, TK_LIST_ENERGY, 4, 1)];
-        k_list_energy<<<grid_for(E->n_sw, tb), tb, 0, s>>>(E->n_sw, E->sw, eng_geo(E), U.bunit, skip, P.ee_f32, P.dhat,
-                                                           P.barrier, P.kappa * P.dt * P.dt, Eo, En);
+        const int grid = dev_count ? NUM_SMS * 4 : grid_for(E->n_sw, tb);
+        k_list_energy<<<grid, tb, 0, s>>>(E->n_sw, dev_count ? &E->dcnt->ls_nsw : nullptr, E->sw, eng_geo(E), U.bunit,
+                                          skip, P.ee_f32, P.dhat, P.barrier, P.kappa * P.dt * P.dt, Eo, En);
         tune_end(E, TK_LIST_ENERGY);
         // per listed pair: the entry, its 2-4 vertex ids and positions
         phase_end(E, ph, E->n_sw * (16.0 + 16.0 + 4 * 24.0));

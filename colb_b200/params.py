@@ -49,6 +49,7 @@ REFERENCE = dict(
     warm_start=0,
     autotune=1,
     ls_groups=0,
+    ls_graph=0,
 )
 
 CONFIG = dict(
@@ -78,6 +79,7 @@ CONFIG = dict(
     warm_start=0,
     autotune=1,
     ls_groups=0,
+    ls_graph=1,
 )
 
 

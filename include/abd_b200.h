@@ -117,7 +117,12 @@ typedef struct AbdParams {
                                groups along the step, so the energy is a sum of independent
                                group energies and each group takes its own CCD bound and
                                back-off).  Convergence stays per scene. */
-    int32_t reserved[4];
+    int32_t ls_graph;       /* 1: run the line-search trials of each Newton iteration as one CUDA
+                               graph whose while-node repeats apply / energy / decide on the
+                               device until every unit has accepted (at most 64 trials), with one
+                               host round trip per search instead of one per trial; 0: the host
+                               loop.  Same kernels and decisions either way. */
+    int32_t reserved[3];
 } AbdParams;
 
 /* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */
@@ -155,7 +160,7 @@ typedef struct AbdStepStats {
     int32_t comp_small;        /*   by the shared-memory dense kernel, */
     int32_t comp_large;        /*   by cuSOLVER (summed over iterations), */
     int32_t krylov_fallbacks;  /*   and solves handed to the Krylov solver */
-    int32_t reserved[1];
+    int32_t ls_graph_launches; /* line searches run as one CUDA graph launch (ls_graph) */
 } AbdStepStats;
 
 typedef struct AbdHandle AbdHandle;
