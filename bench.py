@@ -239,6 +239,7 @@ def run_ours(args, rank, world):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
         eng.step(1)
+    state0 = eng.get_state()      # the end-to-end pass repeats the timed steps from here
     # ---- timed: device time of K steps, L2 flushed before each step
     if world > 1:
         import torch.distributed as dist
@@ -273,19 +274,22 @@ def run_ours(args, rank, world):
         return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
                     lin=lin, e2e_s=float("nan"), clocks=clk.summary(), phases=None, n_timing=0, bytes_state=48 * 8 * eng.nb,
                     graphs=graphs)
-    # ---- e2e through the public API with host buffers: H2D of the state,
-    # one step, D2H of the state every step
-    host_state = eng.get_state()
+    # ---- e2e through the public API with host buffers: the same K steps
+    # from the same state, with H2D of the state, one step and D2H of the
+    # state every step
+    eng.set_state(state0)
     try:
-        pinned = torch.from_numpy(host_state).pin_memory().numpy()
+        pinned = torch.from_numpy(state0.copy()).pin_memory().numpy()
     except Exception:
-        pinned = host_state
+        pinned = state0.copy()
+    e2e_iters = 0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         eng.set_state(pinned)
-        eng.step(1)
-        pinned[:] = eng.get_state()
+        rc, st = eng.step(1)
+        e2e_iters += st.newton_iters
+        eng.get_state(out=pinned)
     e2e_s = time.perf_counter() - t0
     e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -300,7 +304,7 @@ def run_ours(args, rank, world):
     eng.set_timing(False, True)
     return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
                 lin=lin, e2e_s=float(e2e_t.item()), clocks=clk.summary(), phases=phases, n_timing=n_timing,
-                bytes_state=48 * 8 * eng.nb, graphs=graphs)
+                bytes_state=48 * 8 * eng.nb, graphs=graphs, e2e_iters=e2e_iters)
 
 
 def run_forms(args, scenes, p, dev=0):
@@ -429,7 +433,9 @@ def main():
         "gpu_launches": r["launches"],
         "ls_graph_launches": r["graphs"],
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": r["bytes_state"],
-                "d2h_bytes_per_step": r["bytes_state"]},
+                "d2h_bytes_per_step": r["bytes_state"],
+                "newton_iters_per_step": r["e2e_iters"] / (args.steps * len(r["scenes"])),
+                "note": "the timed steps again from the same state, host copies of the state in and out every step"},
         "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic_from_profiles(kernel_names[dom].split(" ")[0], args.workload),

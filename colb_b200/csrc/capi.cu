@@ -151,6 +151,7 @@ void eng_free(Engine* E) {
     void* bd[] = {E->bd_vbeg, E->bd_ebeg, E->bd_tbeg};
     for (void* p : bd) if (p) cudaFree(p);
     grid_free(E->gee); grid_free(E->gpt);
+    if (E->st_in) cudaFree(E->st_in);
     void* ps[] = {E->xbar, E->vbody, E->vscene, E->bscene, E->edges, E->tris, E->mass, E->J, E->planes, E->plane_scene,
                   E->sc_plane_begin, E->sc_body_begin, E->edge_scene, E->tri_scene, E->st, E->backup, E->du, E->g, E->x,
                   E->xf, E->pv, E->ws, E->contacts, E->cst, E->ctype, E->cxb, E->cbody, E->cblk, E->keys, E->keys_s,
@@ -341,12 +342,31 @@ int abd_get_sizes(AbdHandle* h, int32_t* nb, int32_t* nv, int32_t* ne, int32_t* 
     return ABD_OK;
 }
 
+// flags a body whose nxt position (c, q) differs bit for bit from the
+// incoming state
+__global__ void k_positions_differ(int nb, const double* __restrict__ cur, const double* __restrict__ in, int* flag) {
+    GS_LOOP(i, 12L * nb) {
+        long b = i / 12; int k = (int)(i % 12);
+        long o = ST_STRIDE * b + ST_NXT + k;
+        if (__double_as_longlong(cur[o]) != __double_as_longlong(in[o])) *flag = 1;
+    }
+}
+
 int abd_set_state(AbdHandle* h, const double* st, int32_t n) {
     HANDLE(h);
     if (!st || n != E->nb) return E->fail(ABD_ERR_INVALID_ARG, "abd_set_state: n_bodies mismatch");
-    CUDA_TRY(cudaMemcpyAsync(E->st, st, sizeof(double) * 48 * n, cudaMemcpyHostToDevice, E->stream));
+    const size_t bytes = sizeof(double) * 48 * n;
+    if (!E->st_in && cudaMalloc(&E->st_in, bytes) != cudaSuccess) { E->st_in = nullptr; return E->fail(ABD_ERR_CUDA, "cudaMalloc state staging"); }
+    // the swept candidate list covers the current positions: it stays valid
+    // when the caller hands back the positions it read (a host loop that
+    // round-trips the state every step)
+    CUDA_TRY(cudaMemcpyAsync(E->st_in, st, bytes, cudaMemcpyHostToDevice, E->stream));
+    CUDA_TRY(cudaMemsetAsync(&E->dcnt->pos_changed, 0, sizeof(int), E->stream));
+    k_positions_differ<<<grid_for(12L * n), 256, 0, E->stream>>>(n, E->st, E->st_in, &E->dcnt->pos_changed);
+    CUDA_TRY(cudaMemcpyAsync(E->st, E->st_in, bytes, cudaMemcpyDeviceToDevice, E->stream));
+    CUDA_TRY(cudaMemcpyAsync(&E->hcnt->pos_changed, &E->dcnt->pos_changed, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
     CUDA_TRY(cudaStreamSynchronize(E->stream));
-    E->sw_valid = false;
+    if (E->hcnt->pos_changed) E->sw_valid = false;
     return ABD_OK;
 }
 

@@ -92,7 +92,7 @@ struct Counters {
     int overflow, nnzb, n_active, scenes_done;
     int krylov_active, ccd_capped, nan_flag, ls_pending;
     int nkeys, grp_fail, ls_trials, ls_nsw;   // ls_*: trial count and list length of a graph line search
-    int n_sw, n_sw_ee, sw_overflow, pad3;
+    int n_sw, n_sw_ee, sw_overflow, pos_changed;   // pos_changed: abd_set_state moved a body
 };
 #define DETECT_COUNTER_BYTES (5 * sizeof(int))   // n_ee .. overflow
 
@@ -166,6 +166,7 @@ struct Engine {
     float4* grp_lo = nullptr; float4* grp_hi = nullptr;   // [nb]
     void* ls_graph_state = nullptr;   // line-search graphs (ls_graph, step.cu)
     bool capturing = false;           // a graph body is being captured: the autotuner only reports its shape
+    double* st_in = nullptr;          // [48 nb] abd_set_state staging (compared with st before it replaces it)
 
     // cub scratch
     void* cub_tmp = nullptr; size_t cub_bytes = 0;

@@ -141,10 +141,15 @@ class Engine:
         except Exception:
             pass
 
-    def get_state(self):
-        st = np.zeros((self.nb, 48))
-        self._check(self.L.abd_get_state(self.h, _dp(st)))
-        return st
+    def get_state(self, out=None):
+        """(nb, 48) float64 BDFAffine rows; `out` (C-contiguous float64 of that
+        shape, e.g. pinned memory) receives the copy instead of a new array."""
+        if out is None:
+            out = np.zeros((self.nb, 48))
+        elif out.dtype != np.float64 or out.shape != (self.nb, 48) or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("get_state: out must be a C-contiguous float64 array of shape (nb, 48)")
+        self._check(self.L.abd_get_state(self.h, _dp(out)))
+        return out
 
     def set_state(self, st):
         st = np.ascontiguousarray(st, dtype=np.float64).reshape(self.nb, 48)
