@@ -107,8 +107,10 @@ def test_direct_solve_by_components(chain_scene, chain_pairs, hess_mode, precisi
     12 bodies, cuSOLVER above); the result must equal one dense solve."""
     eps = 2.2e-16 if precision == 0 else 1.2e-7
     cases = [(chain_scene, chain_pairs["states"][k]) for k in (1, 2)]
-    net = S.config2_chain_net(n=5, pitch=1.5 - 5e-4, seed=3)
-    cases.append((net, None))
+    # chain mail in contact: 25, 49 and 64 links in one component (the band
+    # solver's window wraps once the component is wider than its band)
+    for n in (5, 7, 8):
+        cases.append((S.config2_chain_net(n=n, pitch=1.5 - 5e-4, seed=3), None))
     for sc, st in cases:
         if st is None:
             p = P.config_params(linear_solver=2, hess_mode=hess_mode, precision=precision)
