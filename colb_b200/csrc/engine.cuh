@@ -222,7 +222,7 @@ enum {
     SD_COUNT
 };
 // per-scene int slots
-enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_STALL, SI_GACT, SI_GSTALL, SI_COUNT };
+enum { SI_DONE = 0, SI_ITER, SI_ACC, SI_KDONE, SI_KITER, SI_NACT, SI_STALL, SI_GACT, SI_GSTALL, SI_DUBAD, SI_COUNT };
 
 // The units the line search runs over: scenes (one step length per scene,
 // the reference's line search) or contact groups (ls_groups).  bunit maps a

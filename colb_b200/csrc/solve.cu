@@ -396,7 +396,45 @@ static int resolved_solver(const Engine* E) {
     return kind;
 }
 
+// Mixed precision: a scene whose FP32 solve left a non-finite entry in du
+// takes the block-Jacobi direction du_b = D_b^-1 g_b instead (every body's
+// inverse diagonal block is finite: a singular block inverts to the
+// identity), so the line search gets a descent direction rather than NaN.
+__global__ void k_du_nonfinite(int nb, const double* __restrict__ du, const int* __restrict__ bscene,
+                               const int* __restrict__ done, int* bad) {
+    GS_LOOP(i, 12L * nb) {
+        int s = bscene[i / 12];
+        if (!done[s] && !isfinite(du[i])) bad[s] = 1;
+    }
+}
+__global__ void k_du_jacobi(int nb, const float* __restrict__ dinv, const double* __restrict__ g,
+                            const int* __restrict__ bscene, const int* __restrict__ bad, double* du) {
+    GS_LOOP(i, 12L * nb) {
+        long b = i / 12; int r = (int)(i % 12);
+        if (!bad[bscene[b]]) continue;
+        const float* D = dinv + 144 * b;
+        double acc = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) acc += (double)D[c * 12 + r] * g[12 * b + c];
+        du[i] = acc;
+    }
+}
+static int du_guard(Engine* E) {
+    cudaStream_t s = E->stream;
+    int* bad = E->sci + SI_DUBAD * E->ns;
+    CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int) * E->ns, s));
+    k_du_nonfinite<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->du, E->bscene, E->sci + SI_DONE * E->ns, bad);
+    k_du_jacobi<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, (const float*)E->dinv, E->g, E->bscene, bad, E->du);
+    E->launches += 2;
+    return ABD_OK;
+}
+static int solve_any(Engine* E, int* iters);
 int eng_solve(Engine* E, int* iters) {
+    int rc = solve_any(E, iters);
+    if (rc || !E->mixed) return rc;
+    return du_guard(E);
+}
+static int solve_any(Engine* E, int* iters) {
     int kind = resolved_solver(E);
     if (kind == ABD_SOLVER_DIRECT) {
         int ph = phase_begin(E, PH_DENSE);

@@ -1,8 +1,8 @@
 """CPU restatement of the learned warm start (test infrastructure only).
 
-The learned warm start has no counterpart in the reference (it is one of the
-additions its north star asks for), so this module restates the library's
-own definitions for the tests to check the CUDA path against:
+The learned warm start has no counterpart in the reference (it is one of
+this library's additions), so this module restates the library's own
+definitions for the tests to check the CUDA path against:
 
 - `features(...)`: the 48 per-body features (include/abd_b200.h, "Learned
   warm start"), from the candidate pairs within ABD_FEAT_RADIUS_DHAT * dhat

@@ -3,7 +3,7 @@
 Bit-exact: vertex transform, candidate pair sets (float32 EE predicate and
 float64 PT / half-space filters).  FP64 tolerances: energy 1e-11 rel,
 gradient / Hessian 1e-9 rel, trajectories 1e-6 rel of the scene extent
-(the north-star FP64 bar).  Mixed precision: 1e-4.
+(the FP64 trajectory tolerance).  Mixed precision: 1e-4.
 """
 import numpy as np
 import pytest
