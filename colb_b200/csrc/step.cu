@@ -151,11 +151,13 @@ static int ls_graph_build(Engine* E, LsGraph& G, const LsUnits& U, const int* ua
     G.shapes[0] = E->tune[TK_LIST_ENERGY].chosen; G.shapes[1] = E->tune[TK_BODY_ENERGY].chosen;
     return ABD_OK;
 }
-// the line search of one Newton iteration as one graph launch; returns
-// ABD_OK with *ran = 0 when the graph cannot be used (the caller then runs
-// the host loop)
+// the line search of one Newton iteration as one graph launch, not waited
+// for: the trial count (dcnt->ls_trials) is read at the Newton bookkeeping's
+// host sync that follows; *body_launches gets the kernels per trial.
+// Returns ABD_OK with *ran = 0 when the graph cannot be used (the caller then
+// runs the host loop).
 static int ls_graph_run(Engine* E, bool groups, const LsUnits& U, const int* uacc, double* ualpha, int* ustall,
-                        int* trials, int* ran) {
+                        int* body_launches, int* ran) {
     *ran = 0;
     if (!E->ls_graph_state) E->ls_graph_state = new LsGraphState();
     auto* S = reinterpret_cast<LsGraphState*>(E->ls_graph_state);
@@ -175,10 +177,8 @@ static int ls_graph_run(Engine* E, bool groups, const LsUnits& U, const int* uac
     }
     k_ls_graph_prep<<<1, 1, 0, E->stream>>>(E->dcnt, E->n_sw);
     CUDA_TRY(cudaGraphLaunch(G.x, E->stream));
-    int rc = eng_sync_counters(E);
-    if (rc) return rc;
-    *trials = E->hcnt->ls_trials;
-    E->launches += 1 + G.body_launches * E->hcnt->ls_trials;
+    E->launches += 1;
+    *body_launches = G.body_launches;
     *ran = 1;
     return ABD_OK;
 }
@@ -362,15 +362,10 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             k_ls_init<<<grid_for(U.n), 256, 0, s>>>(U.n, udone, uacc, ualpha, U.d + SD_TOI * U.n, P.ccd, ustall);
             E->launches++;
             int ph_tr = phase_begin(E, PH_TRIALS);
-            int graph_ran = 0;
+            int graph_ran = 0, graph_body = 0;
             if (P.ls_graph) {
-                int nt = 0;
-                if ((rc = ls_graph_run(E, groups, U, uacc, ualpha, ustall, &nt, &graph_ran))) return rc;
-                if (graph_ran) {
-                    st.ls_trials += nt;
-                    st.ls_graph_launches++;
-                    if (E->hcnt->grp_fail) return E->fail(ABD_ERR_CUDA, "contact groups: union-find did not settle");
-                }
+                if ((rc = ls_graph_run(E, groups, U, uacc, ualpha, ustall, &graph_body, &graph_ran))) return rc;
+                if (graph_ran) st.ls_graph_launches++;
             }
             for (int trial = 0; trial < LS_MAX_TRIALS && !graph_ran; trial++) {
                 k_apply<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->backup, E->du, ualpha, uacc, U.bunit, E->st);
@@ -397,6 +392,12 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
                                             P.newton_tol, E->dcnt);
             E->launches++;
             if ((rc = eng_sync_counters(E))) return rc;
+            if (graph_ran) {
+                // the graph's line search ended before the bookkeeping ran
+                st.ls_trials += E->hcnt->ls_trials;
+                E->launches += graph_body * E->hcnt->ls_trials;
+                if (E->hcnt->grp_fail) return E->fail(ABD_ERR_CUDA, "contact groups: union-find did not settle");
+            }
             if (E->hcnt->nan_flag) return E->fail(ABD_ERR_NAN, "non-finite gradient norm");
             if (E->hcnt->scenes_done == ns) break;
         }
