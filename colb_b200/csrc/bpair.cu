@@ -242,7 +242,8 @@ static int bp_reserve(Engine* E, int bp_need, int key_need) {
         cudaFuncSetAttribute(k_bp_prims, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(4 * BP_CHUNK * sizeof(float4) + 2 * BP_CHUNK * sizeof(int)));
     }
-    cudaStreamSynchronize(E->stream);
+    // buffers in use by queued work are freed only after the stream drains
+    if (bp_need > S->bp_cap || key_need > S->key_cap) cudaStreamSynchronize(E->stream);
     if (bp_need > S->bp_cap) {
         if (S->bpairs) cudaFree(S->bpairs);
         S->bp_cap = bp_need + bp_need / 2 + 1024;
@@ -266,8 +267,10 @@ static int bp_reserve(Engine* E, int bp_need, int key_need) {
 // Build a sorted (kind, a, b) list of EE and PT candidates into `out`
 // (capacity *cap, grown through `grow`).  p may be null (static positions).
 // mode 0: swept list with limit lim; mode 1: detection with distance filt.
+// The list length comes back to the host; its EE count stays on the device
+// (copied to nee_dev when given; BpScratch::cnt[2] until the next build).
 static int bp_build(Engine* E, const double* p, double lim, double filt, int mode, int4*& out, int& cap, int& n_out,
-                    int& n_ee_out, int (*grow)(Engine*, int)) {
+                    int* nee_dev, int (*grow)(Engine*, int)) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
     int rc;
@@ -302,10 +305,8 @@ static int bp_build(Engine* E, const double* p, double lim, double filt, int mod
             k_bp_decode<<<grid_for(n), 256, 0, s>>>(n, S->keys_s, out, S->cnt + 2);
             E->launches += 2;
         }
-        int ne_ = 0;
-        CUDA_TRY(cudaMemcpyAsync(&ne_, S->cnt + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        n_out = n; n_ee_out = ne_;
+        if (nee_dev) CUDA_TRY(cudaMemcpyAsync(nee_dev, S->cnt + 2, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        n_out = n;
         return ABD_OK;
     }
     return E->fail(ABD_ERR_CONTACT_OVERFLOW, "body-pair broad phase did not fit after growing");
@@ -316,15 +317,15 @@ static int grow_ct(Engine* E, int need) { return eng_grow_contacts(E, need); }
 
 // swept list along p = E->pv (computed by the caller), limit lim
 int eng_swept_bp(Engine* E, double lim) {
-    int n = 0, nee = 0;
-    int rc = bp_build(E, E->pv, lim, lim, 0, E->sw, E->sw_cap, n, nee, grow_sw);
+    int n = 0;
+    int rc = bp_build(E, E->pv, lim, lim, 0, E->sw, E->sw_cap, n, E->sw_nee, grow_sw);
     if (rc) return rc;
-    E->n_sw = n; E->n_sw_ee = nee; E->sw_valid = true;
+    E->n_sw = n; E->n_sw_ee = -1; E->sw_valid = true;   // EE count on the device only (E->sw_nee)
     return ABD_OK;
 }
 
-__global__ void k_bp_counts(Counters* cnt, int n_ee, int n) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) { cnt->n_ee = n_ee; cnt->n_pt = n - n_ee; cnt->overflow = 0; }
+__global__ void k_bp_counts(Counters* cnt, const int* __restrict__ n_ee_dev, int n) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) { int n_ee = *n_ee_dev; cnt->n_ee = n_ee; cnt->n_pt = n - n_ee; cnt->overflow = 0; }
 }
 
 // full detection at the current positions with filter filt
@@ -333,9 +334,9 @@ int eng_detect_bp(Engine* E, double filt) {
     if (rc) return rc;
     CUDA_TRY(cudaMemsetAsync(E->dcnt, 0, DETECT_COUNTER_BYTES, E->stream));
     double lim = filt * (1.0 + 1e-6) + 1e-7;
-    int n = 0, nee = 0;
-    if ((rc = bp_build(E, nullptr, lim, filt, 1, E->contacts, E->cap, n, nee, grow_ct))) return rc;
-    k_bp_counts<<<1, 32, 0, E->stream>>>(E->dcnt, nee, n);
+    int n = 0;
+    if ((rc = bp_build(E, nullptr, lim, filt, 1, E->contacts, E->cap, n, nullptr, grow_ct))) return rc;
+    k_bp_counts<<<1, 32, 0, E->stream>>>(E->dcnt, bps(E)->cnt + 2, n);
     E->launches++;
     return eng_pg_candidates(E, filt);
 }

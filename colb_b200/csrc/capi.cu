@@ -117,8 +117,9 @@ int eng_alloc(Engine* E) {
     E->sw_cap = std::max(E->P.contact_capacity, 1024);
     if ((rc = eng_grow_contacts(E, std::max(E->P.contact_capacity, 1024) * 4 / 5))) return rc;
     DALLOC(E->sw, E->sw_cap); DALLOC(E->sw_flag, E->sw_cap + 1); DALLOC(E->sw_off, E->sw_cap + 1);
-    DALLOC(E->pmag, nv); DALLOC(E->zero_int, 1); DALLOC(E->zero_ns, ns);
+    DALLOC(E->pmag, nv); DALLOC(E->zero_int, 1); DALLOC(E->zero_ns, ns); DALLOC(E->sw_nee, 1);
     cudaMemsetAsync(E->zero_int, 0, sizeof(int), E->stream);
+    cudaMemsetAsync(E->sw_nee, 0, sizeof(int), E->stream);
     cudaMemsetAsync(E->zero_ns, 0, sizeof(int) * ns, E->stream);
     DALLOC(E->row_ptr, nb + 1);
     E->blk_cap = 0;
@@ -156,7 +157,7 @@ void eng_free(Engine* E) {
                   E->sc_plane_begin, E->sc_body_begin, E->edge_scene, E->tri_scene, E->st, E->backup, E->du, E->g, E->x,
                   E->xf, E->pv, E->ws, E->contacts, E->cst, E->ctype, E->cxb, E->cbody, E->cblk, E->keys, E->keys_s,
                   E->ukeys, E->row_ptr, E->bcol, E->vals, E->dinv, E->scd, E->sci, E->cub_tmp, E->dcnt, E->prof_d,
-                  E->sw, E->sw_flag, E->sw_off, E->pmag, E->zero_int, E->zero_ns};
+                  E->sw, E->sw_flag, E->sw_off, E->pmag, E->zero_int, E->zero_ns, E->sw_nee};
     for (void* p : ps) if (p) cudaFree(p);
     for (int i = 0; i < 10; i++) if (E->kv[i]) cudaFree(E->kv[i]);
     if (E->hcnt) cudaFreeHost(E->hcnt);

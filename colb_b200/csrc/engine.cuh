@@ -139,6 +139,7 @@ struct Engine {
 
     // swept candidate list (swept.cu)
     int4* sw = nullptr; int sw_cap = 0; int n_sw = 0, n_sw_ee = 0; bool sw_valid = false;
+    int* sw_nee = nullptr;         // device copy of the list's EE count (the list filter reads it)
     int* sw_flag = nullptr; int* sw_off = nullptr;
     float* pmag = nullptr;         // |displacement| per vertex of the listed step
     int* zero_int = nullptr;       // a device 0

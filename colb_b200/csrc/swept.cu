@@ -245,6 +245,7 @@ int eng_swept(Engine* E, const double* dq, double sign, const int* done) {
     }
     E->n_sw = E->hcnt->n_sw;
     E->n_sw_ee = E->hcnt->n_sw_ee;
+    CUDA_TRY(cudaMemcpyAsync(E->sw_nee, &E->dcnt->n_sw_ee, sizeof(int), cudaMemcpyDeviceToDevice, s));
     E->sw_valid = true;
     return ABD_OK;
 }
@@ -381,7 +382,8 @@ __global__ void k_list_flags(int n, const int4* __restrict__ list, Geo G, int f3
     }
 }
 __global__ void k_list_scatter(int n, const int4* __restrict__ list, const int* __restrict__ flag, const int* __restrict__ off,
-                               int4* out, int n_ee_list, Counters* cnt, int cap) {
+                               int4* out, const int* __restrict__ n_ee_dev, Counters* cnt, int cap) {
+    const int n_ee_list = *n_ee_dev;
     GS_LOOP(c, n) {
         if (flag[c]) { int at = off[c]; if (at < cap) out[at] = list[c]; }
     }
@@ -410,7 +412,7 @@ int eng_detect_list(Engine* E) {
         CUDA_TRY(cudaMemsetAsync(flag + n, 0, sizeof(int), s));
         size_t bytes = E->cub_bytes;
         CUDA_TRY(cub::DeviceScan::ExclusiveSum(E->cub_tmp, bytes, flag, off, n + 1, s));
-        k_list_scatter<<<grid_for(n), 256, 0, s>>>(n, E->sw, flag, off, E->contacts, E->n_sw_ee, E->dcnt, E->cap);
+        k_list_scatter<<<grid_for(n), 256, 0, s>>>(n, E->sw, flag, off, E->contacts, E->sw_nee, E->dcnt, E->cap);
         E->launches += 3;
     }
     return eng_pg_candidates(E, P.cand_dist);
