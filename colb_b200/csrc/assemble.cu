@@ -609,7 +609,30 @@ int eng_assemble(Engine* E) {
     int* n_unique = &E->dcnt->nkeys;
     CUDA_TRY(cub::DeviceSelect::Unique(E->cub_tmp, bytes, E->keys_s, E->ukeys, n_unique, nkeys, s));
     E->launches += 4;
+    // the direct solver's component analysis reads the unique keys on the
+    // host: enqueue their copy (the first nkeys >= unique count) so that this
+    // sync covers it
+    E->keys_host = false;
+    const int ls = E->P.linear_solver;
+    const bool direct = ls == ABD_SOLVER_AUTO || ls == ABD_SOLVER_DIRECT;
+    if (direct) {
+        if (nkeys > E->h_ukeys_cap) {
+            if (E->h_ukeys) cudaFreeHost(E->h_ukeys);
+            E->h_ukeys = nullptr; E->h_ukeys_cap = 0;
+            int cap = nkeys + nkeys / 2 + 1024;
+            if (cudaMallocHost(&E->h_ukeys, sizeof(unsigned long long) * cap) != cudaSuccess)
+                return E->fail(ABD_ERR_CUDA, "cudaMallocHost block keys");
+            E->h_ukeys_cap = cap;
+        }
+        if (!E->h_done && cudaMallocHost(&E->h_done, sizeof(int) * E->ns) != cudaSuccess) {
+            E->h_done = nullptr;
+            return E->fail(ABD_ERR_CUDA, "cudaMallocHost done flags");
+        }
+        CUDA_TRY(cudaMemcpyAsync(E->h_ukeys, E->ukeys, sizeof(unsigned long long) * nkeys, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(E->h_done, E->sci + SI_DONE * E->ns, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, s));
+    }
     if ((rc = eng_sync_counters(E))) return rc;
+    E->keys_host = direct;
     int nnzb = E->hcnt->nkeys;   // may include the sentinel
     E->nnzb_host = nnzb;
     if (nnzb > E->blk_cap) { if ((rc = eng_grow_blocks(E, nnzb))) return rc; }

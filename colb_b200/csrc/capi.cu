@@ -153,6 +153,8 @@ void eng_free(Engine* E) {
     for (void* p : bd) if (p) cudaFree(p);
     grid_free(E->gee); grid_free(E->gpt);
     if (E->st_in) cudaFree(E->st_in);
+    if (E->h_ukeys) cudaFreeHost(E->h_ukeys);
+    if (E->h_done) cudaFreeHost(E->h_done);
     void* ps[] = {E->xbar, E->vbody, E->vscene, E->bscene, E->edges, E->tris, E->mass, E->J, E->planes, E->plane_scene,
                   E->sc_plane_begin, E->sc_body_begin, E->edge_scene, E->tri_scene, E->st, E->backup, E->du, E->g, E->x,
                   E->xf, E->pv, E->ws, E->contacts, E->cst, E->ctype, E->cxb, E->cbody, E->cblk, E->keys, E->keys_s,

@@ -18,6 +18,7 @@
 //     Cholesky reports a non-positive pivot).
 // Mixed precision factors in FP32.
 #include "engine.cuh"
+#include <cstring>
 #include <cusolverDn.h>
 #include <algorithm>
 
@@ -695,13 +696,20 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     cudaStream_t st = E->stream;
     const int* ndone = E->sci + SI_DONE * E->ns;
     const int nb = E->nb;
-    // block pattern and done flags to the host
+    // block pattern and done flags to the host (already there when the
+    // assembly copied them within its sync)
     const int nk = E->nnzb_host;
     D->keys.resize(std::max(nk, 1));
     D->done.resize(E->ns);
-    if (nk > 0) CUDA_TRY(cudaMemcpyAsync(D->keys.data(), E->ukeys, sizeof(unsigned long long) * nk, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(D->done.data(), ndone, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    if (E->keys_host && nk <= E->h_ukeys_cap) {
+        if (nk > 0) memcpy(D->keys.data(), E->h_ukeys, sizeof(unsigned long long) * nk);
+        memcpy(D->done.data(), E->h_done, sizeof(int) * E->ns);
+    } else {
+        if (nk > 0) CUDA_TRY(cudaMemcpyAsync(D->keys.data(), E->ukeys, sizeof(unsigned long long) * nk, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(D->done.data(), ndone, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    E->keys_host = false;
     // union-find over bodies, joined by off-diagonal blocks
     std::vector<int>& parent = D->parent;
     parent.resize(nb);

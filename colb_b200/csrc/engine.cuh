@@ -140,6 +140,9 @@ struct Engine {
     // swept candidate list (swept.cu)
     int4* sw = nullptr; int sw_cap = 0; int n_sw = 0, n_sw_ee = 0; bool sw_valid = false;
     int* sw_nee = nullptr;         // device copy of the list's EE count (the list filter reads it)
+    // block keys and done flags of the last assembly, copied to pinned host
+    // memory in the assembly's own sync for the direct solver's analysis
+    unsigned long long* h_ukeys = nullptr; int h_ukeys_cap = 0; int* h_done = nullptr; bool keys_host = false;
     int* sw_flag = nullptr; int* sw_off = nullptr;
     float* pmag = nullptr;         // |displacement| per vertex of the listed step
     int* zero_int = nullptr;       // a device 0
