@@ -308,18 +308,22 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             }
             E->has_ws = 0;
         }
+        bool detected_ahead = false;      // this iteration's list filter ran before the last sync
         for (int it = 0; it < mi; it++) {
             // contact.py:270-279 detection on the current iterate: filter the
             // swept list of the step that led here, or detect from scratch
-            for (;;) {
-                int ph = phase_begin(E, PH_DETECT);
-                rc = E->sw_valid ? eng_detect_list(E) : (eng_use_bp(E) ? eng_detect_bp(E, P.cand_dist) : eng_detect(E, P.cand_dist));
-                phase_end(E, ph, detect_bytes(E));
-                if (rc) return rc;
-                if ((rc = eng_sync_counters(E))) return rc;
+            for (bool ahead = detected_ahead;; ahead = false) {
+                if (!ahead) {
+                    int ph = phase_begin(E, PH_DETECT);
+                    rc = E->sw_valid ? eng_detect_list(E) : (eng_use_bp(E) ? eng_detect_bp(E, P.cand_dist) : eng_detect(E, P.cand_dist));
+                    phase_end(E, ph, detect_bytes(E));
+                    if (rc) return rc;
+                    if ((rc = eng_sync_counters(E))) return rc;
+                }
                 if (!E->hcnt->overflow) break;
                 if ((rc = eng_grow_contacts(E, E->hcnt->n_total))) return rc;
             }
+            detected_ahead = false;
             st.n_pairs = E->hcnt->n_total;
             // abd.py:682-688 assembly
             { int ph = phase_begin(E, PH_ASSEMBLE); rc = eng_assemble(E); phase_end(E, ph, 0); if (rc) return rc; }
@@ -391,7 +395,18 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             k_newton_book<<<1, 256, 0, s>>>(ns, done, iter, stall, E->scd + SD_GG * ns, alpha, prof_res, prof_alpha, mi,
                                             P.newton_tol, E->dcnt);
             E->launches++;
+            // the next iteration's list filter (no host sync inside) is queued
+            // before this sync, which then also brings back its counts; the
+            // filter writes only the detection counters, not the bookkeeping's
+            const bool ahead = E->sw_valid && it + 1 < mi;
+            if (ahead) {
+                int ph = phase_begin(E, PH_DETECT);
+                rc = eng_detect_list(E);
+                phase_end(E, ph, detect_bytes(E));
+                if (rc) return rc;
+            }
             if ((rc = eng_sync_counters(E))) return rc;
+            detected_ahead = ahead;
             if (graph_ran) {
                 // the graph's line search ended before the bookkeeping ran
                 st.ls_trials += E->hcnt->ls_trials;
