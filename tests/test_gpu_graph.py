@@ -58,3 +58,10 @@ def test_graph_rebuilt_when_swept_list_grows():
     sc = S.config2_chain_net(n=3, pitch=1.5 - 5e-4, seed=2)
     graphs, _ = _both(sc, 2, dt=1.0 / 240.0, linear_solver=2, autotune=0, contact_capacity=1)
     assert graphs > 0
+
+
+def test_graph_parameter_is_validated():
+    from colb_b200.engine import AbdError
+    sc = S.config1_cubes(seed=0)
+    with pytest.raises(AbdError):
+        Engine(P.config_params(ls_graph=2), sc)
