@@ -51,6 +51,29 @@ def test_config_sizes():
     assert min(nbs) >= 4 and max(nbs) <= 64
 
 
+def test_pile_config_and_fixture():
+    """4096 icospheres (42 or 162 vertices, radius 0.2..0.5) inside the
+    12 x 12 open box with ground and four walls, no two overlapping at t = 0;
+    the stored benchmark state has the scene's shape and stays in the box."""
+    from colb_b200 import fixtures
+    sc = S.config5_pile()
+    nb = len(sc["mass"])
+    assert nb == 4096 and len(sc["planes"]) == 5
+    counts = np.bincount(sc["vert_body"], minlength=nb)
+    assert set(np.unique(counts)) <= {42, 162}
+    c = sc["state"][:, :3]
+    r = np.array([np.linalg.norm(sc["xbar"][sc["vert_body"] == b], axis=1).max() for b in range(0, nb, 97)])
+    assert r.min() >= 0.2 - 1e-9 and r.max() <= 0.5 + 1e-9
+    assert c[:, 0].min() > 0.0 and c[:, 0].max() < 12.0 and c[:, 2].min() > 0.0 and c[:, 2].max() < 12.0
+    # neighbours on the 1.05 grid: centre distance exceeds the sum of the radii
+    d = np.linalg.norm(c[1] - c[0])
+    assert d > 1.0
+    state, t0, seed = fixtures.load_pile()
+    assert state.shape == (nb, 48) and np.isfinite(state).all() and t0 == 100 and seed == 0
+    cn = state[:, 24:27]
+    assert cn[:, 1].min() > 0.0 and cn[:, 0].min() > 0.0 and cn[:, 0].max() < 12.0
+
+
 def test_load_ma_roundtrip(tmp_path):
     p = tmp_path / "t.ma"
     p.write_text("3 2 1\nv 0 0 0 0.1\nv 1 0 0 0.1\nv 0 1 0 0.1\ne 0 1\ne 1 2\nf 0 1 2\n")
