@@ -207,7 +207,7 @@ def cpu_baseline(scenes, params, cfg, budget_s=20.0, threads=None):
             break
     value = nb * steps / el
     return {"value": value, "unit": "body-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{steps} full steps of {cfg['workload'].split(':')[0]} from t=0 ({el:.1f} s, "
+            "sample": f"{steps} full steps of {cfg['workload'].split(':')[0]} from step {cfg.get('start_step', 0)} ({el:.1f} s, "
                       f"{iters / max(1, steps * len(scenes)):.2f} Newton iters/step/scene), oracle/abd_oracle.c with OpenMP"}
 
 
