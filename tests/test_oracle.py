@@ -140,6 +140,33 @@ def test_gradient_matches_energy_fd(chain_scene, chain_pairs, hess_mode):
     assert np.isfinite(e0)
 
 
+def test_gradient_matches_energy_fd_point_triangle_and_ground():
+    """Two icospheres 0.5 dhat apart (one rotated, so no two edges are
+    parallel), the lower one 0.4 dhat above the ground: point-triangle,
+    edge-edge and half-space contacts with the log barrier; the assembled
+    gradient is the central difference of the oracle energy."""
+    V, F = S.icosphere_mesh(1, 1.0)
+    r, dh = 0.3, 1e-3
+    Va = V * r
+    Vb = Va @ S._rand_rotation(np.random.default_rng(3)).T
+    cA = np.array([0.0, -Va[:, 1].min() + 0.4 * dh, 0.0])
+    cB = cA + Va[np.argmax(Va[:, 1])] - Vb[np.argmin(Vb[:, 1])] + np.array([0.0, 0.5 * dh, 0.0])
+    sc = S.assemble_bodies([S._body(Va, F, 1000.0, cA), S._body(Vb, F, 1000.0, cB)], planes=[S.GROUND])
+    w = O.OracleWorld(P.config_params(), sc)
+    st = w.get_state()
+    _, kinds = w.pairs()
+    assert set(np.unique(kinds)) == {0, 1, 2}
+    g, _ = w.assemble(dense=False)
+    for b in range(2):
+        for k in range(12):
+            h = 1e-7
+            s1, s2 = st.copy(), st.copy()
+            s1[b, 24 + k] += h; s2[b, 24 + k] -= h
+            w.set_state(s1); ep = w.energy()[0]
+            w.set_state(s2); em = w.energy()[0]
+            assert (ep - em) / (2 * h) == pytest.approx(g[12 * b + k], rel=1e-5, abs=1e-6 * np.abs(g).max())
+
+
 def test_reference_chain_steps_converge(chain_scene):
     w = O.OracleWorld(P.reference_params(), chain_scene)
     rc, st = w.step(3)
