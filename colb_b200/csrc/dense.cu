@@ -355,78 +355,67 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         }
         for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = (T)g[12L * ord[e / 12] + e % 12];
         __syncthreads();
-        // D = L_kk L_kk^T in registers (warp 0): lane r < 12 holds row r; the
-        // pivot and its reciprocal square root are computed by every lane
-        // from a broadcast, so the 12 columns need no barrier.  Then
-        // y_k = L_kk^-1 rhs_k.
-        auto factor_diag = [&](int k) {
-            T* D = slot(k, k);
-            T* yk = rhs + (k % BAND_W) * 12;
-            T a[12];
-#pragma unroll
-            for (int c2 = 0; c2 < 12; c2++) a[c2] = lane < 12 ? D[lane * 12 + c2] : (T)0;
-            T rs[12];
-#pragma unroll
-            for (int j = 0; j < 12; j++) {
-                T d = __shfl_sync(0xffffffffu, a[j], j);
-                if (!(d > (T)0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
-                T r = rsqrt_nr(d);
-                rs[j] = r;
-                T l = a[j] * r;                              // L[lane][j] for lane > j
-                if (lane == j) a[j] = d * r;
-                if (lane > j) a[j] = l;
-                // full-range inner loop: every index static, so a[] stays in registers
-#pragma unroll
-                for (int c2 = 0; c2 < 12; c2++) {
-                    T lc = __shfl_sync(0xffffffffu, l, c2);  // L[c2][j] for c2 > j
-                    if (c2 > j && lane > j) a[c2] -= l * lc;
-                }
-            }
-            if (lane < 12) {
-#pragma unroll
-                for (int c2 = 0; c2 < 12; c2++) D[lane * 12 + c2] = c2 <= lane ? a[c2] : (T)0;
-            }
-#pragma unroll
-            for (int j = 0; j < 12; j++) if (lane == j) { rdiag[j] = rs[j]; Rg[(long)k * 12 + j] = rs[j]; }
-            T v = lane < 12 ? yk[lane] : (T)0;
-#pragma unroll
-            for (int t = 0; t < 12; t++) {
-                T yt = __shfl_sync(0xffffffffu, v, t) * rs[t];
-                if (lane == t) v = yt;
-                if (lane > t && lane < 12) v -= a[t] * yt;
-            }
-            if (lane < 12) { yk[lane] = v; du[12L * ord[k] + lane] = (double)v; }
-            __syncwarp();
-        };
-        // warps 1..7 before column k: block row k + wb (fetched during the
-        // previous column) enters the window, block row k + 1 + wb is fetched
-        auto stage_rows = [&](int k) {
-            const int t1 = tid - 32, n1 = blockDim.x - 32;
-            if (k >= 1 && k + wb < N) {
-                const T* src = stage + (k & 1) * BAND_W * 144;
-                for (int e = t1; e < (wb + 1) * 144; e += n1) slot(k + wb, k + e / 144)[e % 144] = src[e];
-            }
-            if (k + 1 + wb < N) {
-                // row k + 1 + wb: block j = k + 1 + q is A(., . - d) with d = wb - q
-                T* dst = stage + ((k + 1) & 1) * BAND_W * 144;
-                const T* src = A + (long)(k + 1 + wb) * BAND_W * 144;
-                for (int e = t1; e < (wb + 1) * 144; e += n1) dst[(wb - e / 144) * 144 + e % 144] = src[e];
-            }
-        };
-        if (warp == 0) factor_diag(0);
-        else stage_rows(0);
-        __syncthreads();
-        // Column k with its diagonal block already factored.  After the panel,
-        // warp 0 applies column k to block (k+1, k+1) and factors it (look-
-        // ahead) while warps 1..7 write the column out, apply it to the rest of
-        // the window, and stage the rows of column k + 1.
         for (int k = 0; k < N; k++) {
             const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
             T* D = slot(k, k);
-            const T* yk = rhs + (k % BAND_W) * 12;
-            // panel: L_ik = A_ik L_kk^-T, one thread per block row (tid < 96);
-            // meanwhile the right-hand side of row k + wb (in the window
-            // since the previous column) is read (tid 128..139)
+            T* yk = rhs + (k % BAND_W) * 12;
+            if (warp == 0) {
+                // D = L_kk L_kk^T in registers: lane r < 12 holds row r; the
+                // pivot and its reciprocal square root are computed by every
+                // lane from a broadcast, so the 12 columns need no barrier
+                T a[12];
+#pragma unroll
+                for (int c2 = 0; c2 < 12; c2++) a[c2] = lane < 12 ? D[lane * 12 + c2] : (T)0;
+                T rs[12];
+#pragma unroll
+                for (int j = 0; j < 12; j++) {
+                    T d = __shfl_sync(0xffffffffu, a[j], j);
+                    if (!(d > (T)0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
+                    T r = rsqrt_nr(d);
+                    rs[j] = r;
+                    T l = a[j] * r;                          // L[lane][j] for lane > j
+                    if (lane == j) a[j] = d * r;
+                    if (lane > j) a[j] = l;
+                    // full-range inner loop: every index static, so a[] stays in registers
+#pragma unroll
+                    for (int c2 = 0; c2 < 12; c2++) {
+                        T lc = __shfl_sync(0xffffffffu, l, c2);   // L[c2][j] for c2 > j
+                        if (c2 > j && lane > j) a[c2] -= l * lc;
+                    }
+                }
+                if (lane < 12) {
+#pragma unroll
+                    for (int c2 = 0; c2 < 12; c2++) D[lane * 12 + c2] = c2 <= lane ? a[c2] : (T)0;
+                }
+#pragma unroll
+                for (int j = 0; j < 12; j++) if (lane == j) { rdiag[j] = rs[j]; Rg[(long)k * 12 + j] = rs[j]; }
+                // y_k = L_kk^-1 rhs_k
+                T v = lane < 12 ? yk[lane] : (T)0;
+#pragma unroll
+                for (int t = 0; t < 12; t++) {
+                    T yt = __shfl_sync(0xffffffffu, v, t) * rs[t];
+                    if (lane == t) v = yt;
+                    if (lane > t && lane < 12) v -= a[t] * yt;
+                }
+                if (lane < 12) { yk[lane] = v; du[12L * ord[k] + lane] = (double)v; }
+            } else {
+                // meanwhile: block row k + wb (fetched during the previous column)
+                // enters the window, and block row k + 1 + wb is fetched
+                const int t1 = tid - 32, n1 = blockDim.x - 32;
+                if (k >= 1 && k + wb < N) {
+                    const T* src = stage + (k & 1) * BAND_W * 144;
+                    for (int e = t1; e < (wb + 1) * 144; e += n1) slot(k + wb, k + e / 144)[e % 144] = src[e];
+                    if (t1 < 12) rhs[((k + wb) % BAND_W) * 12 + t1] = (T)g[12L * ord[k + wb] + t1];
+                }
+                if (k + 1 + wb < N) {
+                    // row k + 1 + wb: block j = k + 1 + q is A(., . - d) with d = wb - q
+                    T* dst = stage + ((k + 1) & 1) * BAND_W * 144;
+                    const T* src = A + (long)(k + 1 + wb) * BAND_W * 144;
+                    for (int e = t1; e < (wb + 1) * 144; e += n1) dst[(wb - e / 144) * 144 + e % 144] = src[e];
+                }
+            }
+            __syncthreads();
+            // panel: L_ik = A_ik L_kk^-T, one thread per block row
             for (int t = tid; t < 12 * nk; t += blockDim.x) {
                 int i = k + 1 + t / 12, r = t % 12;
                 T* R = slot(i, k) + r * 12;
@@ -437,84 +426,52 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 for (int j = 0; j < 12; j++) {
                     T a = x[j];
 #pragma unroll
-                    for (int s2 = 0; s2 < j; s2++) a -= x[s2] * D[j * 12 + s2];
+                    for (int s = 0; s < j; s++) a -= x[s] * D[j * 12 + s];
                     x[j] = a * rdiag[j];
                 }
 #pragma unroll
                 for (int j = 0; j < 12; j++) R[j] = x[j];
             }
-            if (k >= 1 && k + wb < N && tid >= 128 && tid < 140)
-                rhs[((k + wb) % BAND_W) * 12 + tid - 128] = (T)g[12L * ord[k + wb] + tid - 128];
             __syncthreads();
-            if (warp == 0) {
-                if (k + 1 < N) {
-                    // A(k+1, k+1) -= L(k+1, k) L(k+1, k)^T, rhs_{k+1} -= L(k+1, k) y_k
-                    const T* Lr = slot(k + 1, k);
-                    T* Dn = slot(k + 1, k + 1);
-                    for (int e = lane; e < 144; e += 32) {
-                        int r = e / 12, c = e % 12;
-                        T acc = 0;
+            // factor column to global; rhs_i -= L_ik y_k; window update A_ij -= L_ik L_jk^T
+            for (int e = tid; e < (nk + 1) * 144; e += blockDim.x) {
+                int d = e / 144;
+                L[((long)k * BAND_W + d) * 144 + e % 144] = slot(k + d, k)[e % 144];
+            }
+            for (int t = tid; t < 12 * nk; t += blockDim.x) {
+                int i = k + 1 + t / 12, r = t % 12;
+                const T* R = slot(i, k) + r * 12;
+                T acc = 0;
 #pragma unroll
-                        for (int s2 = 0; s2 < 12; s2++) acc += Lr[r * 12 + s2] * Lr[c * 12 + s2];
-                        Dn[e] -= acc;
-                    }
-                    if (lane < 12) {
-                        T acc = 0;
+                for (int c2 = 0; c2 < 12; c2++) acc += R[c2] * yk[c2];
+                rhs[(i % BAND_W) * 12 + r] -= acc;
+            }
+            // A_ij -= L_ik L_jk^T in 3 x 4 tiles (12 per block pair)
+            const int npair = nk * (nk + 1) / 2;
+            for (int e = tid; e < npair * 12; e += blockDim.x) {
+                int p = e / 12, tile = e % 12;
+                int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
+                int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
+                const T* Li = slot(i, k) + r0t * 12;
+                const T* Lj = slot(j, k) + c0t * 12;
+                T acc[3][4] = {};
 #pragma unroll
-                        for (int c2 = 0; c2 < 12; c2++) acc += Lr[lane * 12 + c2] * yk[c2];
-                        rhs[((k + 1) % BAND_W) * 12 + lane] -= acc;
-                    }
-                    __syncwarp();
-                    factor_diag(k + 1);
-                }
-            } else {
-                const int t1 = tid - 32, n1 = blockDim.x - 32;
-                // factor column to global
-                for (int e = t1; e < (nk + 1) * 144; e += n1) {
-                    int d = e / 144;
-                    L[((long)k * BAND_W + d) * 144 + e % 144] = slot(k + d, k)[e % 144];
-                }
-                // rhs_i -= L_ik y_k for i = k+2 .. k+nk
-                for (int t = t1; t < 12 * (nk - 1); t += n1) {
-                    int i = k + 2 + t / 12, r = t % 12;
-                    const T* R = slot(i, k) + r * 12;
-                    T acc = 0;
+                for (int s = 0; s < 12; s++) {
+                    T li[3], lj[4];
 #pragma unroll
-                    for (int c2 = 0; c2 < 12; c2++) acc += R[c2] * yk[c2];
-                    rhs[(i % BAND_W) * 12 + r] -= acc;
-                }
-                // A_ij -= L_ik L_jk^T in 3 x 4 tiles (12 per block pair), all
-                // pairs but (k+1, k+1)
-                const int npair = nk * (nk + 1) / 2;
-                for (int e = t1; e < (npair - 1) * 12; e += n1) {
-                    int p = 1 + e / 12, tile = e % 12;
-                    int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
-                    int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
-                    const T* Li = slot(i, k) + r0t * 12;
-                    const T* Lj = slot(j, k) + c0t * 12;
-                    T acc[3][4] = {};
+                    for (int a2 = 0; a2 < 3; a2++) li[a2] = Li[a2 * 12 + s];
 #pragma unroll
-                    for (int s2 = 0; s2 < 12; s2++) {
-                        T li[3], lj[4];
-#pragma unroll
-                        for (int a2 = 0; a2 < 3; a2++) li[a2] = Li[a2 * 12 + s2];
-#pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) lj[b2] = Lj[b2 * 12 + s2];
-#pragma unroll
-                        for (int a2 = 0; a2 < 3; a2++)
-#pragma unroll
-                            for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
-                    }
-                    T* Aij = slot(i, j);
+                    for (int b2 = 0; b2 < 4; b2++) lj[b2] = Lj[b2 * 12 + s];
 #pragma unroll
                     for (int a2 = 0; a2 < 3; a2++)
 #pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
+                        for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
                 }
-                // the window row that enters next overwrites row k's slots,
-                // whose diagonal block was written out above
-                asm volatile("bar.sync 1, 224;" ::: "memory");
-                if (k + 1 < N) stage_rows(k + 1);
+                T* Aij = slot(i, j);
+#pragma unroll
+                for (int a2 = 0; a2 < 3; a2++)
+#pragma unroll
+                    for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
             }
             __syncthreads();
         }
