@@ -198,17 +198,20 @@ def cpu_baseline(scenes, params, cfg, budget_s=20.0, threads=None):
     nb = dynamic_bodies(scenes)
     steps, t0 = 0, time.perf_counter()
     iters = 0
+    by_step = []
     while True:
         rc, st = w.step(1)
         steps += 1
         iters += st.newton_iters
+        by_step.append(int(st.newton_iters))
         el = time.perf_counter() - t0
         if el > budget_s or steps >= 200:
             break
     value = nb * steps / el
     return {"value": value, "unit": "body-steps/s", "cores": threads, "kind": "port",
             "sample": f"{steps} full steps of {cfg['workload'].split(':')[0]} from step {cfg.get('start_step', 0)} ({el:.1f} s, "
-                      f"{iters / max(1, steps * len(scenes)):.2f} Newton iters/step/scene), oracle/abd_oracle.c with OpenMP"}
+                      f"{iters / max(1, steps * len(scenes)):.2f} Newton iters/step/scene), oracle/abd_oracle.c with OpenMP",
+            "start_step": cfg.get("start_step", 0), "newton_iters_by_step": by_step}
 
 
 def flush_l2(buf):
@@ -237,15 +240,21 @@ def run_ours(args, rank, world):
         eng.set_mlp(params, norm)
     nb = dynamic_bodies(scenes)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    # the warm-up steps settle the autotuner, the line-search graph and the
+    # buffer sizes; the timed steps then start again from the workload's
+    # start state, the same state the CPU arms start from
+    state0 = eng.get_state()
     for _ in range(args.warmup):
         eng.step(1)
-    state0 = eng.get_state()      # the end-to-end pass repeats the timed steps from here
+    eng.set_state(state0)
     # ---- timed: device time of K steps, L2 flushed before each step
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    gpu_ms, launches, iters, unconv, lin, graphs = 0.0, 0, 0, 0, 0, 0
+    gpu_ms, launches, iters, unconv, lin, graphs, syncs = 0.0, 0, 0, 0, 0, 0, 0
+    by_step, xs = [], []
+    keep_x = args.workload == "net16" and not args.profile
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
             flush_l2(flush)
@@ -257,6 +266,10 @@ def run_ours(args, rank, world):
             unconv += st.unconverged
             lin += st.lin_iters
             graphs += st.ls_graph_launches
+            syncs += st.host_syncs
+            by_step.append(int(st.newton_iters))
+            if keep_x and len(xs) < 10:
+                xs.append(eng.vertices())       # after the device-timed step: FP64 positions for the forms' error
     torch.cuda.synchronize()
     t = torch.tensor([gpu_ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -273,7 +286,7 @@ def run_ours(args, rank, world):
     if args.profile:
         return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
                     lin=lin, e2e_s=float("nan"), clocks=clk.summary(), phases=None, n_timing=0, bytes_state=48 * 8 * eng.nb,
-                    graphs=graphs)
+                    graphs=graphs, syncs=syncs, by_step=by_step, state0=state0, xs=xs)
     # ---- e2e through the public API with host buffers: the same K steps
     # from the same state, with H2D of the state, one step and D2H of the
     # state every step
@@ -306,14 +319,19 @@ def run_ours(args, rank, world):
     eng.set_timing(False, True)
     return dict(scenes=scenes, p=p, cfg=cfg, nb=nb, max_ms=max_ms, launches=launches, iters=iters, unconv=unconv,
                 lin=lin, e2e_s=float(e2e_t.item()), clocks=clk.summary(), phases=phases, n_timing=n_timing,
-                bytes_state=48 * 8 * eng.nb, graphs=graphs, e2e_iters=e2e_iters)
+                bytes_state=48 * 8 * eng.nb, graphs=graphs, e2e_iters=e2e_iters, syncs=syncs, by_step=by_step,
+                state0=state0, xs=xs)
 
 
-def run_forms(args, scenes, p, dev=0):
+def run_forms(args, scenes, p, ref_xs=None, dev=0):
     """The three forms beside the plain FP64 solver on the same workload:
     mixed precision, the learned warm start, and 8 scenes batched in one
-    handle (alone and all together).  Device time of min(K, 10) steps after
-    2 warm-up steps, from the same start state."""
+    handle (alone and all together).  Each form warms up for 2 steps, then
+    times min(K, 10) steps from the workload's start state (the plain
+    solver's timed start).  Forms in mixed precision report, for every
+    timed step, the largest vertex position error of the first scene copy
+    against the plain FP64 run's positions after the same step (`ref_xs`),
+    relative to the scene extent."""
     import torch
     from colb_b200 import learned as Lr
     from colb_b200._abi import params_to_dict, params_from_dict
@@ -322,7 +340,8 @@ def run_forms(args, scenes, p, dev=0):
     steps = max(1, min(args.steps, 10))
     base = params_to_dict(p)
     forms = {"mixed": (dict(precision=1), 1, False), "learned": (dict(warm_start=3), 1, True),
-             "batched_x8": ({}, 8, False), "learned+batched_x8+mixed": (dict(precision=1, warm_start=3), 8, True)}
+             "batched_x8": ({}, 8, False), "batched_x8+mixed": (dict(precision=1), 8, False),
+             "learned+batched_x8+mixed": (dict(precision=1, warm_start=3), 8, True)}
     if args.workload == "pile":
         # one scene of 4096 bodies: the batched form steps its contact groups
         # as independent units (one step length per group, ls_groups)
@@ -330,6 +349,7 @@ def run_forms(args, scenes, p, dev=0):
                  "learned": (dict(warm_start=3), 1, True),
                  "learned+contact_groups+mixed": (dict(precision=1, warm_start=3, ls_groups=1), 1, True)}
     out = {}
+    allow = (-5, -6, -7)
     for name, (over, copies, learned) in forms.items():
         e = None
         try:
@@ -337,22 +357,68 @@ def run_forms(args, scenes, p, dev=0):
             if learned:
                 e.set_mlp(params, norm)
             nb = dynamic_bodies(scenes) * copies
+            start = e.get_state()
             for _ in range(2):
-                e.step(1, allow=(-6, -7))
+                e.step(1, allow=allow)
+            e.set_state(start)
             torch.cuda.synchronize()
-            ms = it = unconv = 0
-            for _ in range(steps):
-                rc, st = e.step(1, allow=(-6, -7))
-                ms += st.gpu_ms; it += st.newton_iters; unconv += st.unconverged
+            ms = it = unconv = syncs = 0
+            errs = []
+            nv1 = len(scenes[0]["xbar"])
+            for k in range(steps):
+                rc, st = e.step(1, allow=allow)
+                ms += st.gpu_ms; it += st.newton_iters; unconv += st.unconverged; syncs += st.host_syncs
+                if over.get("precision") == 1 and ref_xs is not None and k < len(ref_xs):
+                    x = e.vertices()[:nv1]
+                    errs.append(float(np.abs(x - ref_xs[k]).max() / np.abs(ref_xs[k]).max()))
             out[name] = {"value": nb * steps / (ms / 1000.0), "unit": "body-steps/s",
                          "newton_iters_per_step": it / (steps * len(scenes) * copies), "unconverged_steps": unconv,
-                         "steps": steps, "intersections": e.count_intersections()}
+                         "steps": steps, "intersections": e.count_intersections(),
+                         "host_syncs_per_step": syncs / steps}
+            if errs:
+                out[name]["max_rel_pos_err_per_step"] = errs
+                out[name]["max_rel_pos_err_vs_fp64"] = max(errs)
         except Exception as ex:                      # report the form as failed, keep the line
             out[name] = {"error": str(ex)}
         finally:
             if e is not None:
                 e.close()
     out["learned_model"] = dict(meta, file="colb_b200/data/warmstart_net16.npz")
+    return out
+
+
+def run_batch512(args, dev=0):
+    """The batched-scenes configuration: 512 scenes of 4..64 cubes / tori in
+    one handle, mixed precision and FP64, device time of min(K, 10) steps
+    after 2 warm-up steps from the scenes' initial state."""
+    import torch
+    from colb_b200 import params as P, scene as S
+    from colb_b200.engine import Engine
+    scenes = S.config3_batch(n_scenes=512, seed=0)
+    nb = dynamic_bodies(scenes)
+    steps = max(1, min(args.steps, 10))
+    out = {"scenes": len(scenes), "bodies": nb}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        e = None
+        try:
+            e = Engine(P.config_params(precision=prec), scenes, device=dev)
+            start = e.get_state()
+            for _ in range(2):
+                e.step(1, allow=(-5, -6, -7))
+            e.set_state(start)
+            torch.cuda.synchronize()
+            ms = it = unconv = 0
+            for _ in range(steps):
+                rc, st = e.step(1, allow=(-5, -6, -7))
+                ms += st.gpu_ms; it += st.newton_iters; unconv += st.unconverged
+            out[name] = {"value": nb * steps / (ms / 1000.0), "unit": "body-steps/s",
+                         "newton_iters_per_step": it / (steps * len(scenes)), "unconverged_steps": unconv,
+                         "steps": steps, "intersections": e.count_intersections()}
+        except Exception as ex:
+            out[name] = {"error": str(ex)}
+        finally:
+            if e is not None:
+                e.close()
     return out
 
 
@@ -431,9 +497,12 @@ def main():
                        l2="flushed before every timed step (256 MB write)", precision="fp64" if args.precision == 0 else "mixed"),
         "newton_iters_per_step": r["iters"] / (args.steps * len(r["scenes"])),
         "krylov_iters_per_step": r["lin"] / args.steps,
+        "newton_iters_by_step": r["by_step"],
+        "timed_steps_start": r["cfg"].get("start_step", 0),
         "unconverged_steps": r["unconv"],
         "gpu_launches": r["launches"],
         "ls_graph_launches": r["graphs"],
+        "host_syncs_per_newton_iter": r["syncs"] / max(1, r["iters"]),
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": r["bytes_state"],
                 "d2h_bytes_per_step": r["bytes_state"],
                 "newton_iters_per_step": r["e2e_iters"] / (args.steps * len(r["scenes"])),
@@ -451,7 +520,17 @@ def main():
     if rank == 0 and world == 1 and args.workload in ("net16", "pile") and not args.no_forms:
         forms = {"plain_fp64": {"value": value, "unit": "body-steps/s",
                                 "newton_iters_per_step": line["newton_iters_per_step"], "steps": args.steps}}
-        forms.update(run_forms(args, r["scenes"], r["p"]))
+        forms.update(run_forms(args, r["scenes"], r["p"], ref_xs=r["xs"]))
+        if args.workload == "net16":
+            forms["batch512"] = run_batch512(args)
+        plain = forms["plain_fp64"]["value"]
+        lbm = forms.get("learned+batched_x8+mixed", {})
+        if "value" in lbm:
+            # the benchmark's headline comparison: learned + batched + mixed
+            # against the plain FP64 solver on the same net, same B200
+            forms["learned+batched_x8+mixed_vs_plain"] = {
+                "speedup": lbm["value"] / plain,
+                "newton_iter_cut": 1.0 - lbm["newton_iters_per_step"] / forms["plain_fp64"]["newton_iters_per_step"]}
         line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if args.workload == "pile":
@@ -459,7 +538,11 @@ def main():
                                     "sample": "none: one oracle step of the 4096-body pile takes longer than 15 min on "
                                               "8 host cores, beyond a bounded sample"}
         else:
-            line["cpu_baseline"] = cpu_baseline(r["scenes"], r["p"], r["cfg"])
+            cb = cpu_baseline(r["scenes"], r["p"], r["cfg"])
+            # both arms start their timed steps from the same state: put the
+            # GPU's Newton iterations of the same steps beside the oracle's
+            cb["gpu_newton_iters_by_step"] = r["by_step"][:len(cb["newton_iters_by_step"])]
+            line["cpu_baseline"] = cb
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -16,6 +16,8 @@ ABD_ERR_NEWTON_CAP = -6
 ABD_ERR_CCD_CAP = -7
 ABD_ERR_NO_DEVICE = -8
 ABD_ERR_NOT_BUILT = -9
+ABD_INJECT_DU_NONFINITE = 1
+ABD_CCD_MAX_ITER = 100000
 
 BARRIER_CUBIC, BARRIER_QUADRATIC, BARRIER_LOG = 0, 1, 2
 HESS_REFERENCE, HESS_PROJECTED = 0, 1
@@ -57,7 +59,9 @@ class AbdParams(C.Structure):
         ("autotune", C.c_int32),
         ("ls_groups", C.c_int32),
         ("ls_graph", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("ccd_max_iter", C.c_int32),
+        ("test_inject", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
 
@@ -98,10 +102,14 @@ class AbdStepStats(C.Structure):
         ("comp_large", C.c_int32),
         ("krylov_fallbacks", C.c_int32),
         ("ls_graph_launches", C.c_int32),
+        ("solver_capped", C.c_int32),
+        ("du_guard_hits", C.c_int32),
+        ("host_syncs", C.c_int32),
+        ("reserved_stats", C.c_int32),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved_stats"}
 
 
 def params_from_dict(d):

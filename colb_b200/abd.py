@@ -12,9 +12,12 @@ Differences from the reference, all deliberate:
     inertia blocks of bodies 4i..4i+3);
   * the contact list is sorted and grows on demand instead of wrapping at
     10000 entries (contact.py:8, :137);
-  * the linear solve is a block-Jacobi preconditioned BiCGSTAB (or PCG),
-    not Warp's unpreconditioned bicgstab; both stop at the same relative
-    tolerance.
+  * the linear solve (ABD_SOLVER_AUTO) is a direct solve per connected
+    component of the contact graph (banded block Cholesky, shared-memory
+    dense factorization, or block-Jacobi preconditioned BiCGSTAB / PCG when
+    the components are too large), not Warp's unpreconditioned bicgstab;
+    the reference's own solver_config="cg" choice maps to
+    ABD_SOLVER_BICGSTAB, which stops at the same relative tolerance.
 """
 import json
 import os
@@ -63,9 +66,11 @@ class Soup:
 class NewtonAbd:
     """NewtonAbd(h, config_file) as in abd.py:584.  `config_file` may be a
     reference JSON scene (e.g. assets/chains.json), an .npz scene written by
-    colb_b200.scene.save_npz_scene, or a scene dict."""
+    colb_b200.scene.save_npz_scene, or a scene dict.  The profiler records
+    `frames` frames of at most newton_max_iter iterations, like the
+    reference's Profiller(max_iters=16, frames=50) (abd.py:599)."""
 
-    def __init__(self, h, config_file, params=None, device=0, frames=4000):
+    def __init__(self, h, config_file, params=None, device=0, frames=50):
         if isinstance(config_file, dict):
             sc = config_file
         elif str(config_file).endswith(".npz"):

@@ -561,7 +561,7 @@ __global__ void k_grad_norm(int nb, const double* __restrict__ g, const int* __r
 
 int eng_sync_counters(Engine* E) {
     CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, E->stream));
-    CUDA_TRY(cudaStreamSynchronize(E->stream));
+    CUDA_TRY(eng_stream_sync(E));
     return ABD_OK;
 }
 

@@ -243,7 +243,7 @@ static int bp_reserve(Engine* E, int bp_need, int key_need) {
                              (int)(4 * BP_CHUNK * sizeof(float4) + 2 * BP_CHUNK * sizeof(int)));
     }
     // buffers in use by queued work are freed only after the stream drains
-    if (bp_need > S->bp_cap || key_need > S->key_cap) cudaStreamSynchronize(E->stream);
+    if (bp_need > S->bp_cap || key_need > S->key_cap) eng_stream_sync(E);
     if (bp_need > S->bp_cap) {
         if (S->bpairs) cudaFree(S->bpairs);
         S->bp_cap = bp_need + bp_need / 2 + 1024;
@@ -292,7 +292,7 @@ static int bp_build(Engine* E, const double* p, double lim, double filt, int mod
         E->launches += 3;
         int h[2];
         CUDA_TRY(cudaMemcpyAsync(h, S->cnt, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
+        CUDA_TRY(eng_stream_sync(E));
         if (h[0] > S->bp_cap || h[1] > S->key_cap) {
             if ((rc = bp_reserve(E, h[0], h[1]))) return rc;
             continue;

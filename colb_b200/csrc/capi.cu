@@ -3,6 +3,7 @@
 #include "contact.cuh"
 #include <cub/cub.cuh>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -196,6 +197,7 @@ void abd_default_params(AbdParams* p) {
     p->contact_capacity = 1 << 16;
     p->pinned_diag = 100.0;                       // abd.py:146
     p->autotune = 1;
+    p->ccd_max_iter = ABD_CCD_MAX_ITER;
 }
 
 const char* abd_last_error(AbdHandle* h) {
@@ -215,7 +217,8 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     const AbdParams& P = *params;
     if (!(P.dt > 0) || !(P.dhat > 0) || !(P.cand_dist >= P.dhat) || P.newton_max_iter <= 0 || P.lin_max_iter <= 0 ||
         P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || P.linear_solver < 0 || P.linear_solver > 3 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1)) ||
-        P.ls_groups < 0 || P.ls_groups > 1 || P.ls_graph < 0 || P.ls_graph > 1) {
+        P.ls_groups < 0 || P.ls_groups > 1 || P.ls_graph < 0 || P.ls_graph > 1 || P.ccd_max_iter < 0 ||
+        (P.test_inject & ~ABD_INJECT_DU_NONFINITE)) {
         g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale, ls_groups, ls_graph)";
         return ABD_ERR_INVALID_ARG;
     }
@@ -358,6 +361,10 @@ __global__ void k_positions_differ(int nb, const double* __restrict__ cur, const
 int abd_set_state(AbdHandle* h, const double* st, int32_t n) {
     HANDLE(h);
     if (!st || n != E->nb) return E->fail(ABD_ERR_INVALID_ARG, "abd_set_state: n_bodies mismatch");
+    for (long i = 0; i < 48L * n; i++)
+        if (!std::isfinite(st[i]))
+            return E->fail(ABD_ERR_NAN, "abd_set_state: non-finite value at body " + std::to_string(i / 48) +
+                                        ", entry " + std::to_string(i % 48) + " (state left unchanged)");
     const size_t bytes = sizeof(double) * 48 * n;
     if (!E->st_in && cudaMalloc(&E->st_in, bytes) != cudaSuccess) { E->st_in = nullptr; return E->fail(ABD_ERR_CUDA, "cudaMalloc state staging"); }
     // the swept candidate list covers the current positions: it stays valid
@@ -550,10 +557,12 @@ int abd_solve(AbdHandle* h, double* du, int32_t* iters) {
     int rc = assemble_full(E);
     if (rc) return rc;
     int it = 0;
+    E->solver_capped = 0;
     if ((rc = eng_solve(E, &it))) return rc;
     CUDA_TRY(cudaMemcpyAsync(du, E->du, sizeof(double) * 12 * E->nb, cudaMemcpyDeviceToHost, E->stream));
     CUDA_TRY(cudaStreamSynchronize(E->stream));
     if (iters) *iters = it;
+    if (E->solver_capped) return E->fail(ABD_ERR_SOLVER_CAP, "abd_solve: Krylov iteration cap reached above tolerance");
     return ABD_OK;
 }
 

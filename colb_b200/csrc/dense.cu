@@ -664,7 +664,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     } else {
         if (nk > 0) CUDA_TRY(cudaMemcpyAsync(D->keys.data(), E->ukeys, sizeof(unsigned long long) * nk, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaMemcpyAsync(D->done.data(), ndone, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
+        CUDA_TRY(eng_stream_sync(E));
     }
     E->keys_host = false;
     // union-find over bodies, joined by off-diagonal blocks
@@ -896,7 +896,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
                     return E->fail(ABD_ERR_CUDA, "cusolver potrf");
             std::vector<int> info(2 * nlarge);
             CUDA_TRY(cudaMemcpyAsync(info.data(), D->info + 2, sizeof(int) * 2 * nlarge, cudaMemcpyDeviceToHost, st));
-            CUDA_TRY(cudaStreamSynchronize(st));
+            CUDA_TRY(eng_stream_sync(E));
             for (int c = 0; c < nlarge; c++) {
                 if (info[2 * c] != 0) {
                     // not positive definite after all: rebuild this component for LU

@@ -580,7 +580,7 @@ __global__ void k_vertex_disp(int nv, const int* __restrict__ vbody, const doubl
 
 __global__ void k_ccd_ee(int ne, GridView GV, Geo G, const double* __restrict__ p, const float4* __restrict__ qlo,
                          const float4* __restrict__ qhi, const int* __restrict__ qscene, int self_contact,
-                         double s_ccd, const int* done, double* toi, int* capped) {
+                         double s_ccd, int ccd_it, const int* done, double* toi, int* capped) {
     GS_LOOP(i, ne) {
         int s = qscene[i];
         if (done[s]) continue;
@@ -595,14 +595,14 @@ __global__ void k_ccd_ee(int ne, GridView GV, Geo G, const double* __restrict__ 
             double xx[12], pp[12];
             for (int k = 0; k < 4; k++) for (int c = 0; c < 3; c++) { xx[3*k+c] = G.x[3*v[k]+c]; pp[3*k+c] = p[3*v[k]+c]; }
             double t;
-            if (accd(0, xx, pp, s_ccd, best, &t, capped) && t < best) best = t;
+            if (accd(0, xx, pp, s_ccd, best, &t, capped, ccd_it) && t < best) best = t;
         });
         if (best < 1.0) atomic_min_pos(toi + s, best);
     }
 }
 __global__ void k_ccd_pt(int nv, GridView GV, Geo G, const double* __restrict__ p, const float4* __restrict__ qlo,
                          const float4* __restrict__ qhi, const int* __restrict__ qscene, int self_contact,
-                         double s_ccd, const int* done, double* toi, int* capped) {
+                         double s_ccd, int ccd_it, const int* done, double* toi, int* capped) {
     GS_LOOP(pi, nv) {
         int s = qscene[pi];
         if (done[s]) continue;
@@ -616,7 +616,7 @@ __global__ void k_ccd_pt(int nv, GridView GV, Geo G, const double* __restrict__ 
             double xx[12], pp[12];
             for (int k = 0; k < 4; k++) for (int q = 0; q < 3; q++) { xx[3*k+q] = G.x[3*v[k]+q]; pp[3*k+q] = p[3*v[k]+q]; }
             double tt;
-            if (accd(1, xx, pp, s_ccd, best, &tt, capped) && tt < best) best = tt;
+            if (accd(1, xx, pp, s_ccd, best, &tt, capped, ccd_it) && tt < best) best = tt;
         });
         if (best < 1.0) atomic_min_pos(toi + s, best);
     }
@@ -657,7 +657,7 @@ int eng_ccd(Engine* E, const double* dq, double sign) {
         E->launches++;
         if ((rc = eng_grid_build(E, g))) return rc;
         k_ccd_ee<<<grid_for(E->ne, 64), 64, 0, s>>>(E->ne, eng_view(g), G, E->pv, g.lo, g.hi, g.scene, P.self_contact, P.ccd_scale,
-                                                    done, toi, &E->dcnt->ccd_capped);
+                                                    ccd_iters(P), done, toi, &E->dcnt->ccd_capped);
         E->launches++;
     }
     if (P.contact_pt && E->nt > 0) {
@@ -668,7 +668,7 @@ int eng_ccd(Engine* E, const double* dq, double sign) {
         E->launches += 2;
         if ((rc = eng_grid_build(E, g))) return rc;
         k_ccd_pt<<<grid_for(E->nv, 64), 64, 0, s>>>(E->nv, eng_view(g), G, E->pv, g.qlo, g.qhi, g.qscene, P.self_contact, P.ccd_scale,
-                                                    done, toi, &E->dcnt->ccd_capped);
+                                                    ccd_iters(P), done, toi, &E->dcnt->ccd_capped);
         E->launches++;
     }
     if (E->npl > 0) {
@@ -715,7 +715,7 @@ int eng_intersections(Engine* E, int* count) {
     k_intersections<<<grid_for(E->ne, 128), 128, 0, s>>>(E->ne, eng_view(g), geo(E), q.lo, q.hi, q.scene, &E->dcnt->nkeys);
     E->launches += 3;
     CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(eng_stream_sync(E));
     *count = E->hcnt->nkeys;
     return ABD_OK;
 }

@@ -93,6 +93,7 @@ struct Counters {
     int krylov_active, ccd_capped, nan_flag, ls_pending;
     int nkeys, grp_fail, ls_trials, ls_nsw;   // ls_*: trial count and list length of a graph line search
     int n_sw, n_sw_ee, sw_overflow, pos_changed;   // pos_changed: abd_set_state moved a body
+    int du_guard;                                  // mixed-precision increments replaced (du_guard)
 };
 #define DETECT_COUNTER_BYTES (5 * sizeof(int))   // n_ee .. overflow
 
@@ -105,6 +106,9 @@ struct Engine {
     std::string err;
     int launches = 0;
     int comp_band = 0, comp_small = 0, comp_large = 0, krylov_fallbacks = 0;   // direct-solver counters
+    int solver_capped = 0;         // Krylov solves that ended at lin_max_iter above tolerance
+    int du_guard_hits = 0;         // mixed-precision increments replaced by the block-Jacobi direction
+    int host_syncs = 0;            // stream synchronisations of the current call
     struct Tuner {
         int chosen = -1, next = 0, running = -1;
         float sum[8] = {0}; int cnt[8] = {0};
@@ -236,6 +240,12 @@ struct LsUnits { int n; const int* bunit; double* d; int* i; };
 inline LsUnits scene_units(Engine* E) { return LsUnits{E->ns, E->bscene, E->scd, E->sci}; }
 inline LsUnits group_units(Engine* E) { return LsUnits{E->nb, E->grp, E->gscd, E->gsci}; }
 
+// a host round trip on the handle's stream, counted for AbdStepStats.host_syncs
+inline cudaError_t eng_stream_sync(Engine* E) { E->host_syncs++; return cudaStreamSynchronize(E->stream); }
+
+// iteration cap of one additive-CCD query
+inline int ccd_iters(const AbdParams& P) { return P.ccd_max_iter > 0 ? P.ccd_max_iter : ABD_CCD_MAX_ITER; }
+
 // launch helpers
 inline int grid_for(long n, int block = 256) {
     long g = (n + block - 1) / block;
@@ -275,7 +285,7 @@ int eng_transform(Engine* E);
 int eng_detect(Engine* E, double filt);               // sorted candidate list at the nxt state
 int eng_energy(Engine* E, int slot);                   // per-scene energy into scd[slot]
 int eng_assemble(Engine* E);                           // g and blocks at the nxt state (uses the candidate list)
-int eng_solve(Engine* E, int* iters);                  // du = A^-1 g for scenes not done
+int eng_solve(Engine* E, int* iters, bool first_iter = false);   // du = A^-1 g for scenes not done
 int eng_solve_direct(Engine* E, int* iters, int* fallback);   // dense factorization per connected component
 void eng_dense_free(Engine* E);
 void eng_features_free(Engine* E);

@@ -211,7 +211,7 @@ extern "C" int abd_get_features(AbdHandle* h, float* feat, int32_t n) {
     int rc = eng_features(E, d);
     if (!rc) {
         cudaError_t e = cudaMemcpyAsync(feat, d, sizeof(float) * 48 * (size_t)E->nb, cudaMemcpyDeviceToHost, E->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
+        if (e == cudaSuccess) e = eng_stream_sync(E);
         if (e != cudaSuccess) rc = E->fail(ABD_ERR_CUDA, std::string("abd_get_features: ") + cudaGetErrorString(e));
     }
     cudaFree(d);

@@ -378,7 +378,7 @@ static int mlp_check(Engine* E) {
     MlpDev* M = reinterpret_cast<MlpDev*>(E->mlp);
     int h = 0;
     CUDA_TRY(cudaMemcpyAsync(&h, M->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
-    CUDA_TRY(cudaStreamSynchronize(E->stream));
+    CUDA_TRY(eng_stream_sync(E));
     if (h) return E->fail(ABD_ERR_CUDA, "mlp inference: a wait ran out");
     return ABD_OK;
 }
@@ -453,7 +453,7 @@ extern "C" int abd_set_mlp(AbdHandle* h, const float* params, const float* norm)
     if (e == cudaSuccess) e = cudaMemcpyAsync(M->norm, norm, sizeof(float) * ABD_MLP_NNORM, cudaMemcpyHostToDevice, E->stream);
     if (e == cudaSuccess) {
         k_mlp_pack<<<grid_for((long)MH * MH), 256, 0, E->stream>>>(P, reinterpret_cast<__nv_bfloat16*>(M->pack), M->bias);
-        e = cudaStreamSynchronize(E->stream);
+        e = eng_stream_sync(E);
     }
     cudaFree(P);
     if (e != cudaSuccess) return E->fail(ABD_ERR_CUDA, std::string("abd_set_mlp: ") + cudaGetErrorString(e));
@@ -479,7 +479,7 @@ extern "C" int abd_mlp_forward(AbdHandle* h, const float* x, int32_t n, float* y
     if (!rc) rc = mlp_check(E);
     if (!rc) {
         e = cudaMemcpyAsync(y, dy, sizeof(float) * MO * (size_t)n, cudaMemcpyDeviceToHost, E->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
+        if (e == cudaSuccess) e = eng_stream_sync(E);
         if (e != cudaSuccess) rc = E->fail(ABD_ERR_CUDA, "abd_mlp_forward: copy out");
     }
     cudaFree(dx); cudaFree(dy);

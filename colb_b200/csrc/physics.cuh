@@ -432,14 +432,15 @@ DV double d2_pt_plane_full(d3 p, d3 t0, d3 t1, d3 t2, double* g, double* H) {
 // ------------------------------------------------------------ additive CCD
 // kind 0: edge-edge (x0 x1 | x2 x3), kind 1: point-triangle (x0 | x1 x2 x3).
 // Returns 1 on a hit with *toi = conservative time; 0 if none in [0,tmax].
-// The iteration count is capped; on the cap the time reached so far is
-// returned (conservative) and *capped is set.
-#define ACCD_MAX_ITERS 100000
+// The iteration count is capped at max_iter (AbdParams.ccd_max_iter, or
+// ABD_CCD_MAX_ITER); on the cap the time reached so far is returned
+// (conservative) and *capped is set.
 DV double prim_dist2(int kind, const double* x) {
     if (kind == 0) { double s, t, d; seg_seg_f64(x, x + 3, x + 6, x + 9, 0.0, s, t, d); return d * d; }
     return pt_dist2(x, x + 3, x + 6, x + 9);
 }
-DV int accd(int kind, const double* x0, const double* p0, double s, double tmax, double* toi, int* capped) {
+DV int accd(int kind, const double* x0, const double* p0, double s, double tmax, double* toi, int* capped,
+            int max_iter) {
     double x[12], p[12], pm[3] = {0, 0, 0};
     for (int i = 0; i < 12; i++) { x[i] = x0[i]; p[i] = p0[i]; }
     for (int i = 0; i < 4; i++) for (int k = 0; k < 3; k++) pm[k] += p[3*i+k] * 0.25;
@@ -452,7 +453,7 @@ DV int accd(int kind, const double* x0, const double* p0, double s, double tmax,
     if (d == 0.0) { *toi = 0.0; return 1; }
     double g = s * d;
     double t = 0, tl = (1 - s) * d / lp;
-    for (int it = 0; it < ACCD_MAX_ITERS; it++) {
+    for (int it = 0; it < max_iter; it++) {
         for (int i = 0; i < 12; i++) x[i] += tl * p[i];
         d = sqrt(prim_dist2(kind, x));
         if (t > 0 && d < g) { *toi = t; return 1; }

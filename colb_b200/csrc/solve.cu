@@ -377,11 +377,13 @@ static int solve_t(Engine* E, int* iters) {
             if (E->hcnt->krylov_active == 0) { k++; break; }
         }
     }
+    // the cap ended the solve with scenes above tolerance: reported, not fatal
+    if (k >= A.maxit && E->hcnt->krylov_active > 0) E->solver_capped++;
     k_copy_out<T><<<grid_for(12L * nb), 256, 0, st>>>(12 * nb, kv[KV_X], E->du);
     E->launches++;
     // iterations actually used by the slowest scene
     CUDA_TRY(cudaMemcpyAsync(E->hsci, kiter, sizeof(int) * ns, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    CUDA_TRY(eng_stream_sync(E));
     int mx = 0;
     for (int s = 0; s < ns; s++) mx = E->hsci[s] > mx ? E->hsci[s] : mx;
     *iters = mx;
@@ -419,20 +421,39 @@ __global__ void k_du_jacobi(int nb, const float* __restrict__ dinv, const double
         du[i] = acc;
     }
 }
-static int du_guard(Engine* E) {
+// counts the scenes whose increment the guard replaced (read with the
+// step's statistics, no sync of its own)
+__global__ void k_du_guard_count(int ns, const int* __restrict__ bad, Counters* cnt) {
+    int n = 0;
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) n += bad[s];
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(&cnt->du_guard, n);
+}
+// test hook (AbdParams.test_inject): a non-finite increment in scene 0,
+// written over the solver's output on the host's request; no kernel reads
+// outside du
+__global__ void k_du_poison(const int* __restrict__ bscene, int nb, double* du) {
+    GS_LOOP(i, 12L * nb) if (bscene[i / 12] == 0 && (i % 12) == 0) du[i] = __longlong_as_double(0x7ff8000000000000LL);
+}
+static int du_guard(Engine* E, bool inject) {
     cudaStream_t s = E->stream;
     int* bad = E->sci + SI_DUBAD * E->ns;
+    if (inject) {
+        k_du_poison<<<grid_for(12L * E->nb), 256, 0, s>>>(E->bscene, E->nb, E->du);
+        E->launches++;
+    }
     CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int) * E->ns, s));
     k_du_nonfinite<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->du, E->bscene, E->sci + SI_DONE * E->ns, bad);
     k_du_jacobi<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, (const float*)E->dinv, E->g, E->bscene, bad, E->du);
-    E->launches += 2;
+    k_du_guard_count<<<1, 256, 0, s>>>(E->ns, bad, E->dcnt);
+    E->launches += 3;
     return ABD_OK;
 }
 static int solve_any(Engine* E, int* iters);
-int eng_solve(Engine* E, int* iters) {
+int eng_solve(Engine* E, int* iters, bool first_iter) {
     int rc = solve_any(E, iters);
     if (rc || !E->mixed) return rc;
-    return du_guard(E);
+    return du_guard(E, first_iter && (E->P.test_inject & ABD_INJECT_DU_NONFINITE));
 }
 static int solve_any(Engine* E, int* iters) {
     int kind = resolved_solver(E);

@@ -8,16 +8,21 @@
 // buffers for its inputs and outputs, and every intermediate (boxes, grid
 // keys, buckets, per-edge counts, radix-sort and scan scratch) lives in the
 // file-scope __device__ arrays below, sized for ABD_STATIC_MAX_EDGES edges.
-// Every GPU that loads the library holds these arrays (about 6 MB) until the
-// process exits.
+// Every GPU that loads the library holds these arrays until the process
+// exits: boxes 2 MiB, grid keys and values 1 MiB, buckets 1 MiB, per-edge
+// counts and offsets 0.5 MiB, sort and scan scratch 4 MiB, about 8.5 MiB in
+// all.
 //
 // Host code must not pass the arrays' names to a kernel: in host code a
 // __device__ symbol names a host-side stand-in, not device memory.  The
 // first call on each device, with that device current, looks the device
 // addresses up with cudaGetSymbolAddress and caches them; make that first
-// call before any stream capture.  All calls share the arrays: two calls
-// whose work overlaps on the GPU (different streams, or the same arrays used
-// by two threads at once) race and corrupt each other's results.
+// call before any stream capture.  The cache is not refreshed: after a
+// cudaDeviceReset of a device, this entry point must not be called on that
+// device again in the same process.  Every call waits for its stream before
+// it returns (it reads the pair count back).  All calls share the arrays:
+// two calls whose work overlaps on the GPU (different streams, or the same
+// arrays used by two threads at once) race and corrupt each other's results.
 #include "engine.cuh"
 #include "physics.cuh"
 #include <cub/cub.cuh>
@@ -34,7 +39,7 @@ static __device__ __align__(256) float4 g_st_hi[ST_MAXE];
 static __device__ __align__(256) uint32_t g_st_keys[2 * ST_MAXE];
 static __device__ __align__(256) int g_st_vals[2 * ST_MAXE];
 static __device__ __align__(256) int g_st_bucket[2 * ST_H];
-static __device__ __align__(256) int g_st_count[2 * (ST_MAXE + 1) + 4];   // counts, offsets, overflow flag
+static __device__ __align__(256) int g_st_count[2 * (ST_MAXE + 1) + 4];   // counts, offsets, bad-edge flag
 static __device__ __align__(256) float g_st_cell[4];
 static __device__ __align__(256) unsigned char g_st_cub[ST_CUB_BYTES];
 
@@ -101,10 +106,13 @@ __global__ void k_st_ranges(int n, const uint32_t* __restrict__ keys, int* bstar
         if (i == n - 1 || keys[i+1] != k) bend[k] = (int)i + 1;
     }
 }
-// mode 0: count per edge; mode 1: write vertex quadruples, sorted by partner
+// mode 0: count per edge; mode 1: write vertex quadruples, sorted by
+// partner, the rows that fit below cap (an edge whose rows cross cap keeps
+// the ones it visited first, so on overflow the rows are not the first cap
+// rows of the complete sorted list)
 __global__ void k_st_pairs(int ne, GridView GV, const double* __restrict__ x, const int* __restrict__ edges,
                            const float4* __restrict__ qlo, const float4* __restrict__ qhi, double cand, int mode,
-                           int* count, const int* off, int* out4, int cap, int* overflow) {
+                           int* count, const int* off, int* out4, int cap) {
     float fc = __double2float_rn(cand);
     GS_LOOP(i, ne) {
         int ii = (int)i;
@@ -125,7 +133,6 @@ __global__ void k_st_pairs(int ne, GridView GV, const double* __restrict__ x, co
                 // the partner edge index goes in slot 2 until the segment is sorted
                 int at = base + c;
                 if (at < cap) { out4[4*at] = a0; out4[4*at+1] = a1; out4[4*at+2] = j; out4[4*at+3] = -1; }
-                else *overflow = 1;
             }
             c++;
         });
@@ -149,9 +156,8 @@ __global__ void k_st_pairs(int ne, GridView GV, const double* __restrict__ x, co
 __global__ void k_st_check(int ne, const int* __restrict__ edges, int nv, int* bad) {
     GS_LOOP(i, 2L * ne) { int v = edges[i]; if (v < 0 || v >= nv) *bad = 1; }
 }
-__global__ void k_st_total(const int* off, int ne, int* n_out, int* flag) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) { *n_out = off[ne]; }
-    (void)flag;
+__global__ void k_st_total(const int* off, int ne, int* n_out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *n_out = off[ne];
 }
 
 extern "C" int abd_ee_pairs_static(const double* x_dev, const int32_t* edges_dev, int32_t n_verts, int32_t n_edges,
@@ -172,17 +178,17 @@ extern "C" int abd_ee_pairs_static(const double* x_dev, const int32_t* edges_dev
     cudaStream_t s = (cudaStream_t)stream_ptr;
     // clear what the previous call left behind
     float* cell = S->cell;
-    int* overflow = S->count + 2 * (ST_MAXE + 1);
+    int* bad_edge = S->count + 2 * (ST_MAXE + 1);
     if (cudaMemsetAsync(cell, 0, sizeof(float), s) != cudaSuccess ||
-        cudaMemsetAsync(overflow, 0, sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(bad_edge, 0, sizeof(int), s) != cudaSuccess ||
         cudaMemsetAsync(n_pairs_dev, 0, sizeof(int32_t), s) != cudaSuccess) {
         err = "abd_ee_pairs_static: cudaMemsetAsync failed"; return ABD_ERR_CUDA;
     }
     if (n_edges < 2) return cudaStreamSynchronize(s) == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
     {
         int bad = 0;
-        k_st_check<<<grid_for(2L * n_edges), 256, 0, s>>>(n_edges, edges_dev, n_verts, overflow);
-        if (cudaMemcpyAsync(&bad, overflow, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        k_st_check<<<grid_for(2L * n_edges), 256, 0, s>>>(n_edges, edges_dev, n_verts, bad_edge);
+        if (cudaMemcpyAsync(&bad, bad_edge, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) { err = "abd_ee_pairs_static: CUDA error"; return ABD_ERR_CUDA; }
         if (bad) { err = "abd_ee_pairs_static: an edge index is outside [0, n_verts)"; return ABD_ERR_INVALID_ARG; }
     }
@@ -207,17 +213,16 @@ extern "C" int abd_ee_pairs_static(const double* x_dev, const int32_t* edges_dev
     k_st_ranges<<<grid_for(n_edges), 256, 0, s>>>(n_edges, keys_s, bstart, bend);
     GridView GV{S->lo, S->hi, nullptr, cell, vals_s, bstart, bend, (uint32_t)(H - 1)};
     k_st_pairs<<<grid_for(n_edges, 128), 128, 0, s>>>(n_edges, GV, x_dev, edges_dev, S->lo, S->hi, cand_dist, 0, count,
-                                                      nullptr, pairs_dev, cap, overflow);
+                                                      nullptr, pairs_dev, cap);
     if (cudaMemsetAsync(count + n_edges, 0, sizeof(int), s) != cudaSuccess) { err = "abd_ee_pairs_static: memset"; return ABD_ERR_CUDA; }
     if (cub::DeviceScan::ExclusiveSum(S->cub, need2, count, off, n_edges + 1, s) != cudaSuccess) {
         err = "abd_ee_pairs_static: scan failed"; return ABD_ERR_CUDA;
     }
     k_st_pairs<<<grid_for(n_edges, 128), 128, 0, s>>>(n_edges, GV, x_dev, edges_dev, S->lo, S->hi, cand_dist, 1, count,
-                                                      off, pairs_dev, cap, overflow);
-    k_st_total<<<1, 32, 0, s>>>(off, n_edges, n_pairs_dev, overflow);
-    int n = 0, of = 0;
+                                                      off, pairs_dev, cap);
+    k_st_total<<<1, 32, 0, s>>>(off, n_edges, n_pairs_dev);
+    int n = 0;
     if (cudaMemcpyAsync(&n, n_pairs_dev, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaMemcpyAsync(&of, overflow, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         err = std::string("abd_ee_pairs_static: ") + cudaGetErrorString(cudaGetLastError());
         return ABD_ERR_CUDA;

@@ -271,6 +271,8 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     AbdStepStats st; memset(&st, 0, sizeof st); st.min_toi = 1.0;
     int launches0 = E->launches;
     E->comp_band = E->comp_small = E->comp_large = E->krylov_fallbacks = 0;
+    E->solver_capped = 0; E->host_syncs = 0;
+    int ccd_capped = 0;
     CUDA_TRY(cudaEventRecord(E->ev0, s));
     for (int step = 0; step < n_steps; step++) {
         CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int) * ns, s));
@@ -329,7 +331,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             { int ph = phase_begin(E, PH_ASSEMBLE); rc = eng_assemble(E); phase_end(E, ph, 0); if (rc) return rc; }
             // abd.py:690 / :631-658 solve
             int li = 0;
-            { int ph = phase_begin(E, PH_SOLVE); rc = eng_solve(E, &li); phase_end(E, ph, 0); if (rc) return rc; }
+            { int ph = phase_begin(E, PH_SOLVE); rc = eng_solve(E, &li, it == 0); phase_end(E, ph, 0); if (rc) return rc; }
             st.lin_iters += li;
             st.n_active = E->hcnt->n_active;
             // candidates along x -> x - J du, shared by CCD, every energy
@@ -416,6 +418,9 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             if (E->hcnt->nan_flag) return E->fail(ABD_ERR_NAN, "non-finite gradient norm");
             if (E->hcnt->scenes_done == ns) break;
         }
+        // counters of this step (the last bookkeeping sync brought them back)
+        st.du_guard_hits += E->hcnt->du_guard;
+        ccd_capped |= E->hcnt->ccd_capped;
         if (P.ccd) {
             double* toi = E->scd + SD_TOI * ns;
             CUDA_TRY(cudaMemcpyAsync(E->hscd, toi, sizeof(double) * ns, cudaMemcpyDeviceToHost, s));
@@ -428,7 +433,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
         CUDA_TRY(cudaMemcpyAsync(hr.data(), prof_res, sizeof(double) * ns * mi, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaMemcpyAsync(ha.data(), prof_alpha, sizeof(double) * ns * mi, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaMemcpyAsync(hi.data(), iter, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
+        CUDA_TRY(eng_stream_sync(E));
         for (int sc = 0; sc < ns; sc++) {
             int n = hi[sc];
             for (int k = 0; k < n; k++) {
@@ -454,7 +459,11 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
     st.kernel_launches = E->launches - launches0;
     st.comp_band = E->comp_band; st.comp_small = E->comp_small; st.comp_large = E->comp_large;
     st.krylov_fallbacks = E->krylov_fallbacks;
+    st.solver_capped = E->solver_capped;
+    st.host_syncs = E->host_syncs + 1;      // + the closing event synchronisation
     if (stats) *stats = st;
-    if (E->hcnt->ccd_capped) return E->fail(ABD_ERR_CCD_CAP, "CCD iteration cap reached (step clamped conservatively)");
+    if (ccd_capped) return E->fail(ABD_ERR_CCD_CAP, "CCD iteration cap reached (step clamped conservatively)");
+    if (E->solver_capped)
+        return E->fail(ABD_ERR_SOLVER_CAP, "Krylov iteration cap reached above tolerance (step taken with that increment)");
     return ABD_OK;
 }

@@ -252,8 +252,8 @@ int eng_swept(Engine* E, const double* dq, double sign, const int* done) {
 
 // ------------------------------------------------------------------ CCD over the list
 __global__ void k_ccd_list(int n, const int4* __restrict__ list, Geo G, const double* __restrict__ p,
-                           const int* __restrict__ bscene, const int* __restrict__ skip, double s_ccd, double* toi,
-                           int* capped) {
+                           const int* __restrict__ bscene, const int* __restrict__ skip, double s_ccd, int ccd_it,
+                           double* toi, int* capped) {
     GS_LOOP(c, n) {
         int4 C = list[c];
         int v[4];
@@ -265,7 +265,7 @@ __global__ void k_ccd_list(int n, const int4* __restrict__ list, Geo G, const do
         double xx[12], pp[12];
         for (int k = 0; k < 4; k++) for (int q = 0; q < 3; q++) { xx[3*k+q] = G.x[3*v[k]+q]; pp[3*k+q] = p[3*v[k]+q]; }
         double t;
-        if (accd(kind, xx, pp, s_ccd, 1.0, &t, capped)) atomic_min_pos(toi + s, t);
+        if (accd(kind, xx, pp, s_ccd, 1.0, &t, capped, ccd_it)) atomic_min_pos(toi + s, t);
     }
 }
 // planes come from the vertex's scene; the bound goes to the unit of its body
@@ -297,8 +297,8 @@ int eng_ccd_list(Engine* E, const LsUnits& U, const int* skip) {
     if (rc) return rc;
     Geo G = eng_geo(E);
     if (E->n_sw > 0)
-        k_ccd_list<<<grid_for(E->n_sw, 64), 64, 0, s>>>(E->n_sw, E->sw, G, E->pv, U.bunit, skip, E->P.ccd_scale, toi,
-                                                        &E->dcnt->ccd_capped);
+        k_ccd_list<<<grid_for(E->n_sw, 64), 64, 0, s>>>(E->n_sw, E->sw, G, E->pv, U.bunit, skip, E->P.ccd_scale,
+                                                        ccd_iters(E->P), toi, &E->dcnt->ccd_capped);
     if (E->npl > 0) k_ccd_pg2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, G, E->pv, E->vscene, U.bunit, E->P.ccd_scale, skip, toi);
     E->launches += 1 + (E->n_sw > 0) + (E->npl > 0);
     return ABD_OK;

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define ABD_ABI_VERSION 1
+#define ABD_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------- */
 #define ABD_LS_STALL_ALPHA 1e-6
@@ -122,8 +122,18 @@ typedef struct AbdParams {
                                device until every unit has accepted (at most 64 trials), with one
                                host round trip per search instead of one per trial; 0: the host
                                loop.  Same kernels and decisions either way. */
-    int32_t reserved[3];
+    int32_t ccd_max_iter;   /* iteration cap of one additive-CCD query (0: ABD_CCD_MAX_ITER); a
+                               query that reaches it returns the time reached so far (a
+                               conservative bound) and the step reports ABD_ERR_CCD_CAP */
+    int32_t test_inject;    /* host-side failure injection for tests, 0 in production:
+                               ABD_INJECT_DU_NONFINITE overwrites the first Newton increment of
+                               every step of scene 0 with NaN before the mixed-precision guard
+                               runs (the guard must replace it by the block-Jacobi direction) */
+    int32_t reserved[1];
 } AbdParams;
+
+#define ABD_CCD_MAX_ITER 100000
+#define ABD_INJECT_DU_NONFINITE 1
 
 /* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */
 typedef struct AbdSceneDesc {
@@ -161,6 +171,12 @@ typedef struct AbdStepStats {
     int32_t comp_large;        /*   by cuSOLVER (summed over iterations), */
     int32_t krylov_fallbacks;  /*   and solves handed to the Krylov solver */
     int32_t ls_graph_launches; /* line searches run as one CUDA graph launch (ls_graph) */
+    int32_t solver_capped;     /* Krylov solves that stopped at lin_max_iter above lin_tol
+                                  (abd_step then returns ABD_ERR_SOLVER_CAP, non-fatal) */
+    int32_t du_guard_hits;     /* mixed precision: scene solves whose increment had a non-finite
+                                  entry and were replaced by the block-Jacobi direction */
+    int32_t host_syncs;        /* host round trips (stream synchronisations) of the call */
+    int32_t reserved_stats;
 } AbdStepStats;
 
 typedef struct AbdHandle AbdHandle;
@@ -323,13 +339,18 @@ int abd_get_timing(AbdHandle* h, double* ms, int64_t* launches, double* bytes);
  * quadruples (a1, a2, b1, b2), but takes DEVICE pointers: x_dev (n_verts*3
  * doubles), edges_dev (n_edges*2 ints), pairs_dev (cap*4 ints) and
  * n_pairs_dev (one int).  All scratch lives in static device arrays of the
- * library sized for ABD_STATIC_MAX_EDGES edges; larger inputs are rejected
- * with ABD_ERR_INVALID_ARG.  The first call on each device looks those
- * arrays up (make it before any stream capture).  Calls share the arrays:
- * calls whose GPU work overlaps race.  Work runs on `stream` (a
- * cudaStream_t, NULL for the legacy default stream) and the call returns
- * after synchronising it; ABD_ERR_CONTACT_OVERFLOW if more than cap pairs
- * exist (*n_pairs_dev holds the full count).  Errors: abd_last_error(NULL). */
+ * library (about 8.5 MiB per GPU, held until exit) sized for
+ * ABD_STATIC_MAX_EDGES edges; larger inputs are rejected with
+ * ABD_ERR_INVALID_ARG.  The first call on each device looks those arrays up
+ * and caches their addresses (make it before any stream capture; after a
+ * cudaDeviceReset of that device, do not call this entry point on it again
+ * in the same process).  Calls share the arrays: calls whose GPU work
+ * overlaps race.  Work runs on `stream` (a cudaStream_t, NULL for the
+ * legacy default stream) and the call waits for that stream before it
+ * returns.  ABD_ERR_CONTACT_OVERFLOW if more than cap pairs exist:
+ * *n_pairs_dev holds the full count, nothing is written at or beyond row
+ * cap, and which pairs the first cap rows hold is unspecified.
+ * Errors: abd_last_error(NULL). */
 #define ABD_STATIC_MAX_EDGES (1 << 16)
 int abd_ee_pairs_static(const double* x_dev, const int32_t* edges_dev, int32_t n_verts, int32_t n_edges,
                         double cand_dist, int32_t* pairs_dev, int32_t cap, int32_t* n_pairs_dev, void* stream);

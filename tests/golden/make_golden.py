@@ -2,6 +2,8 @@
 assets.  Run in a checkout where the reference (Luke-Skycrawler/colb) is
 mounted; the GPU-side tests only read the .npz files written here.
 
+Usage: COLB_REFERENCE=<reference checkout> python tests/golden/make_golden.py
+
   chains_scene.npz   assets/chains.json + assets/link.ma of the reference,
                      loaded the way utils/scene.py:55-85 and medial.py:17-51
                      do (rest vertices rotated by the xyz Euler angles and
@@ -26,7 +28,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", ".."))
-REF = os.environ.get("COLB_REFERENCE", "/root/reference")
+# the checkout of the reference whose assets/ the fixtures are built from;
+# there is no default, so the script never reads a path it was not given
+REF = os.environ.get("COLB_REFERENCE")
 
 
 def seg_seg_f32(p1, q1, p2, q2, eps=np.float32(1e-6)):
@@ -119,4 +123,6 @@ def main():
 
 
 if __name__ == "__main__":
+    if not REF:
+        sys.exit("set COLB_REFERENCE to the reference checkout (the directory holding assets/chains.json)")
     main()

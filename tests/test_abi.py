@@ -31,7 +31,7 @@ def test_library_exports_every_symbol(built_library):
     L = load_library(built_library)
     for name in header_functions():
         assert hasattr(L, name), name
-    assert L.abd_abi_version() == 1
+    assert L.abd_abi_version() == 2
 
 
 def test_default_params_are_reference_constants(built_library):
@@ -71,6 +71,8 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", offsetof(AbdParams, lin_tol), offsetof(AbdParams, precision),
          offsetof(AbdParams, pinned_diag), offsetof(AbdParams, warm_start));
   printf("%zu %zu\n", offsetof(AbdSceneDesc, planes), offsetof(AbdStepStats, gpu_ms));
+  printf("%zu %zu %zu %zu\n", offsetof(AbdParams, ccd_max_iter), offsetof(AbdParams, test_inject),
+         offsetof(AbdStepStats, solver_capped), offsetof(AbdStepStats, host_syncs));
   return 0; }
 '''
     with tempfile.TemporaryDirectory() as d:
@@ -82,5 +84,7 @@ int main(void) {
     got = [int(v) for v in out]
     want = [C.sizeof(_abi.AbdParams), C.sizeof(_abi.AbdSceneDesc), C.sizeof(_abi.AbdStepStats),
             _abi.AbdParams.lin_tol.offset, _abi.AbdParams.precision.offset, _abi.AbdParams.pinned_diag.offset,
-            _abi.AbdParams.warm_start.offset, _abi.AbdSceneDesc.planes.offset, _abi.AbdStepStats.gpu_ms.offset]
+            _abi.AbdParams.warm_start.offset, _abi.AbdSceneDesc.planes.offset, _abi.AbdStepStats.gpu_ms.offset,
+            _abi.AbdParams.ccd_max_iter.offset, _abi.AbdParams.test_inject.offset,
+            _abi.AbdStepStats.solver_capped.offset, _abi.AbdStepStats.host_syncs.offset]
     assert got == want

@@ -224,17 +224,21 @@ def test_contact_capacity_grows(chain_scene, chain_pairs, broadphase):
 
 
 def test_invalid_arguments_return_errors(chain_scene):
+    import ctypes
     from colb_b200.engine import AbdError
     with pytest.raises(AbdError):
         Engine(P.reference_params(dhat=-1.0), chain_scene)
     e = Engine(P.reference_params(), chain_scene)
-    rc = e.L.abd_set_state(e.h, np.zeros((e.nb, 48)).ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)),
-                           e.nb + 1)
+    st = np.zeros((e.nb + 1, 48))
+    rc = e.L.abd_set_state(e.h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), e.nb + 1)
     assert rc == -1 and b"mismatch" in e.L.abd_last_error(e.h)
-    with pytest.raises(AbdError):
-        e.set_warm_start(np.zeros((e.nb, 12)))  # features path is fine; warm start of the wrong size below
-        e.L  # noqa: B018
-        raise AbdError(-1, "sentinel")
+    # a warm start whose body count differs from the handle's
+    ws = np.zeros((e.nb + 1, 12), dtype=np.float32)
+    rc = e.L.abd_set_warm_start(e.h, ws.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), e.nb + 1)
+    assert rc == -1 and b"mismatch" in e.L.abd_last_error(e.h)
+    rc = e.L.abd_set_warm_start(e.h, None, e.nb)
+    assert rc == -1
+    e.set_warm_start(np.zeros((e.nb, 12)))   # the right size is accepted
 
 
 def test_net_trajectory_matches_oracle():
