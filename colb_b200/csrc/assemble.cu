@@ -559,7 +559,21 @@ __global__ void k_grad_norm(int nb, const double* __restrict__ g, const int* __r
     }
 }
 
+// waits for the copy the last assembly queued (counters, block keys, done
+// flags), not for the assembly kernels behind it
+int eng_asm_wait(Engine* E) {
+    if (!E->asm_pending) return ABD_OK;
+    E->asm_pending = false;
+    E->host_syncs++;
+    CUDA_TRY(cudaEventSynchronize(E->ev_asm));
+    E->keys_host = E->asm_direct;
+    E->nnzb_host = E->hcnt->nkeys;   // may include the sentinel
+    return ABD_OK;
+}
+
 int eng_sync_counters(Engine* E) {
+    int rc = eng_asm_wait(E);
+    if (rc) return rc;
     CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, E->stream));
     CUDA_TRY(eng_stream_sync(E));
     return ABD_OK;
@@ -596,6 +610,11 @@ int eng_assemble(Engine* E) {
     // counters were synchronised by the caller after detection
     int n = E->hcnt->n_total;
     int nkeys = nb + 2 * n;
+    // room for every block before the count is known: the unique keys are
+    // at most the nkeys written and at most every scene's dense pattern,
+    // plus the sentinel
+    const long long bound = std::min<long long>(nkeys, E->dense_blocks) + 1;
+    if (bound > E->blk_cap) { if ((rc = eng_grow_blocks(E, (int)bound))) return rc; }
     int ph = phase_begin(E, PH_ASM_KEYS);
     CUDA_TRY(cudaMemsetAsync(&E->dcnt->n_active, 0, sizeof(int), s));
     k_diag_keys<<<grid_for(nb), 256, 0, s>>>(nb, E->keys);
@@ -610,8 +629,9 @@ int eng_assemble(Engine* E) {
     CUDA_TRY(cub::DeviceSelect::Unique(E->cub_tmp, bytes, E->keys_s, E->ukeys, n_unique, nkeys, s));
     E->launches += 4;
     // the direct solver's component analysis reads the unique keys on the
-    // host: enqueue their copy (the first nkeys >= unique count) so that this
-    // sync covers it
+    // host: enqueue their copy (the first nkeys >= unique count) with the
+    // counters behind one event; the assembly kernels are queued after it
+    // and run while the host waits for the keys (eng_asm_wait)
     E->keys_host = false;
     const int ls = E->P.linear_solver;
     const bool direct = ls == ABD_SOLVER_AUTO || ls == ABD_SOLVER_DIRECT;
@@ -631,11 +651,11 @@ int eng_assemble(Engine* E) {
         CUDA_TRY(cudaMemcpyAsync(E->h_ukeys, E->ukeys, sizeof(unsigned long long) * nkeys, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaMemcpyAsync(E->h_done, E->sci + SI_DONE * E->ns, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, s));
     }
-    if ((rc = eng_sync_counters(E))) return rc;
-    E->keys_host = direct;
-    int nnzb = E->hcnt->nkeys;   // may include the sentinel
-    E->nnzb_host = nnzb;
-    if (nnzb > E->blk_cap) { if ((rc = eng_grow_blocks(E, nnzb))) return rc; }
+    CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(E->ev_asm, s));
+    E->asm_pending = true;
+    E->asm_direct = direct;
+    const long nnzb = bound;     // launch bound; the kernels read the count from the device
     k_block_rows<<<grid_for(nnzb), 256, 0, s>>>(nb, E->ukeys, n_unique, E->row_ptr, E->bcol, E->dcnt);
     phase_end(E, ph, 0);
     double sc = P.kappa * P.dt * P.dt;
@@ -659,6 +679,7 @@ int eng_assemble(Engine* E) {
         int p2 = phase_begin(E, PH_ASM_CONTACT);
         if (n > 0)
             launch_contact_assemble<double>(E, n, G, sc, V);
+        if (E->timing && (rc = eng_asm_wait(E))) return rc;    // n_active for the phase's bytes
         // per candidate: type; per active contact: stencil, barrier argument,
         // 4 positions + 4 rest positions, 4 body blocks and the gradient rows
         phase_end(E, p2, 4.0 * n + E->hcnt->n_active * (16.0 + 8.0 + 96.0 + 96.0 + 4 * 1152.0 + 384.0));

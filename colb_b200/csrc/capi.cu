@@ -139,6 +139,7 @@ int eng_alloc(Engine* E) {
     cudaMemsetAsync(E->sci, 0, sizeof(int) * SI_COUNT * ns, E->stream);
     cudaMemsetAsync(E->dcnt, 0, sizeof(Counters), E->stream);
     cudaEventCreate(&E->ev0); cudaEventCreate(&E->ev1);
+    cudaEventCreateWithFlags(&E->ev_asm, cudaEventDisableTiming);
     return ABD_OK;
 }
 
@@ -168,6 +169,7 @@ void eng_free(Engine* E) {
     if (E->hsci) cudaFreeHost(E->hsci);
     if (E->ev0) cudaEventDestroy(E->ev0);
     if (E->ev1) cudaEventDestroy(E->ev1);
+    if (E->ev_asm) cudaEventDestroy(E->ev_asm);
     if (E->stream) cudaStreamDestroy(E->stream);
 }
 
@@ -267,6 +269,10 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     }
     E->nb = nb; E->nv = nv; E->ne = (int)escene.size(); E->nt = (int)tscene.size(); E->npl = npl;
     E->h_body_begin = sc_body_begin;
+    for (int s = 0; s < n_scenes; s++) {
+        long long m = sc_body_begin[s + 1] - sc_body_begin[s];
+        E->dense_blocks += m * m;
+    }
     E->h_bscene = bscene;
     E->h_edges = edges; E->h_tris = tris;
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) { delete E; g_err = "stream"; return ABD_ERR_CUDA; }
@@ -516,7 +522,8 @@ static int assemble_full(Engine* E) {
     CUDA_TRY(cudaMemsetAsync(E->sci + SI_DONE * E->ns, 0, sizeof(int) * E->ns, E->stream));
     int rc = detect_full(E);
     if (rc) return rc;
-    return eng_assemble(E);
+    if ((rc = eng_assemble(E))) return rc;
+    return eng_asm_wait(E);
 }
 
 int abd_assemble(AbdHandle* h, double* grad, double* hess) {
@@ -528,8 +535,8 @@ int abd_assemble(AbdHandle* h, double* grad, double* hess) {
     CUDA_TRY(cudaMemcpyAsync(grad, E->g, sizeof(double) * 12 * E->nb, cudaMemcpyDeviceToHost, E->stream));
     CUDA_TRY(cudaStreamSynchronize(E->stream));
     if (hess) {
-        int nnzb = E->hcnt->nkeys;
         if ((rc = eng_sync_counters(E))) return rc;
+        int nnzb;
         nnzb = E->hcnt->nnzb;
         std::vector<int> rp(E->nb + 1), col(nnzb);
         size_t es = E->mixed ? 4 : 8;

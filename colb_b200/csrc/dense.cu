@@ -270,15 +270,33 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_solve(int nsmall, const
 // ------------------------------------------------------------------ band components
 // A component whose bodies, in reverse Cuthill-McKee order, couple only
 // bodies at most BAND_MAX apart is a block band matrix: its Cholesky factor
-// has the same band.  One CTA factors it with a sliding window of
-// (BAND_MAX + 1)^2 12x12 blocks in shared memory (block column k: factor the
-// diagonal block, solve the panel below, update the window, load the next
-// block row), eliminating the right-hand side on the way (L y = g); the
-// factor's block columns go to global scratch for the backward solve
-// L^T du = y.  No host synchronisation, all band components in one launch.
+// L has the same band.  One CTA factors it with a sliding window of
+// (BAND_MAX + 1)^2 12x12 blocks in shared memory, all band components in
+// one launch, with no host synchronisation.  Block column k takes two
+// phases, each closed by a block barrier:
+//   1. panel: L_ik = A_ik Linv_k^T for the blocks below the diagonal, where
+//      Linv_k = L_kk^-1 is kept explicitly, so every entry is an
+//      independent dot product; forward elimination y_k = Linv_k g_k;
+//   2. warp 0 applies column k to the next diagonal block
+//      (A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T), factors it in registers and
+//      inverts the factor (Linv_{k+1}), while warps 1..7 apply column k to
+//      the rest of the window (A_ij -= L_ik L_jk^T), eliminate the
+//      right-hand sides below, write the factor column to global scratch
+//      and bring the next block row into the window.
+// The 12 dependent pivots of each diagonal block thereby run beside the
+// trailing update instead of before it.  The backward solve walks the
+// columns again: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).
+// The factorization runs in FP64 in both precision modes: a mixed-precision
+// handle gathers its FP32 blocks into FP64, because FP32 roundings of a
+// stiff projected Hessian can make a pivot non-positive and the band path
+// has no pivoting fallback.
 constexpr int BAND_MAX = 8;
 constexpr int BAND_W = BAND_MAX + 1;
 constexpr int BAND_THREADS = 256;
+// shared-memory stride of one 12x12 block: 146 doubles put the 81 block
+// bases of the window on different banks (144 would start every block on
+// bank 0, and tiles of different blocks read by one warp would conflict)
+constexpr int BAND_BLK = 146;
 
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
 constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
@@ -295,16 +313,16 @@ DV double rsqrt_nr(double d) {
     r = r * (1.5 - h * r * r);
     return r;
 }
-DV float rsqrt_nr(float d) { return rsqrtf(d); }
 
-// Band blocks of every band component, contiguous: A(i, i - d) of position
-// i (component order), d = 0..BAND_MAX, row-major, at (loff + i BAND_W + d);
-// blocks outside the band or absent are zero.  One warp per block.
-template <class T>
+// Band blocks of every band component, contiguous and in FP64: A(i, i - d)
+// of position i (component order), d = 0..BAND_MAX, row-major, at
+// (loff + i BAND_W + d); blocks outside the band or absent are zero.  One
+// warp per block.
+template <class TV>
 __global__ void k_band_gather(int npos, const int* __restrict__ pcomp, const int* __restrict__ cptr,
                               const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
-                              const int* __restrict__ row_ptr, const int* __restrict__ bcol, const T* __restrict__ vals,
-                              T* Ab) {
+                              const int* __restrict__ row_ptr, const int* __restrict__ bcol, const TV* __restrict__ vals,
+                              double* Ab) {
     const int lane = threadIdx.x & 31;
     for (long item = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < (long)npos * BAND_W;
          item += ((long)gridDim.x * blockDim.x) >> 5) {
@@ -312,29 +330,80 @@ __global__ void k_band_gather(int npos, const int* __restrict__ pcomp, const int
         int c = pcomp[p], i = p - cptr[c], j = i - d;
         int bi = -1;
         if (j >= 0 && d <= cbw[c]) bi = find_block(row_ptr, bcol, order[p], order[cptr[c] + j]);
-        T* dst = Ab + (loff[c] + (long)i * BAND_W + d) * 144;
+        double* dst = Ab + (loff[c] + (long)i * BAND_W + d) * 144;
         for (int e = lane; e < 144; e += 32) {
             int r = e / 12, cc = e % 12;
-            dst[e] = bi >= 0 ? vals[(long)bi * 144 + cc * 12 + r] : (T)0;     // row-major from column-major
+            dst[e] = bi >= 0 ? (double)vals[(long)bi * 144 + cc * 12 + r] : 0.0;     // row-major from column-major
         }
     }
 }
 
-template <class T>
+// Warp-wide: Cholesky factor of the 12x12 SPD block D (row-major, stride
+// BAND_BLK, lower triangle read), written back into D's lower triangle, and
+// its inverse Linv = L^-1 (row-major 12x12, zeros above the diagonal).  Lane
+// r holds row r; each pivot is broadcast, its reciprocal square root computed
+// by every lane, so the 12 columns need no barrier.  A non-positive pivot
+// sets bit 1 of *status and is replaced by its magnitude.
+DV void band_factor_inverse(double* D, double* linv, int* status) {
+    const int lane = threadIdx.x & 31;
+    double a[12], rs[12];
+#pragma unroll
+    for (int c = 0; c < 12; c++) a[c] = lane < 12 ? D[lane * BAND_BLK + c] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+        double d = __shfl_sync(0xffffffffu, a[j], j);
+        if (!(d > 0.0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + 1e-30; }
+        double r = rsqrt_nr(d);
+        rs[j] = r;
+        double l = a[j] * r;                      // L[lane][j] for lane > j
+        if (lane == j) a[j] = d * r;
+        if (lane > j) a[j] = l;
+        // every index static, so a[] stays in registers
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            double lc = __shfl_sync(0xffffffffu, l, c);   // L[c][j] for c > j
+            if (c > j && lane > j) a[c] -= l * lc;
+        }
+    }
+    if (lane < 12) {
+#pragma unroll
+        for (int c = 0; c < 12; c++) if (c <= lane) D[lane * BAND_BLK + c] = a[c];
+    }
+    __syncwarp();
+    // column `lane` of L^-1 by forward substitution, L[r][s] broadcast from
+    // shared memory: x[r] = (delta(r, lane) - sum_{s<r} L[r][s] x[s]) / L[r][r]
+    double x[12];
+#pragma unroll
+    for (int r = 0; r < 12; r++) {
+        double acc0 = (lane == r) ? 1.0 : 0.0, acc1 = 0.0;
+#pragma unroll
+        for (int s = 0; s < r; s++) {
+            double Lrs = D[r * BAND_BLK + s];
+            if (s & 1) acc1 -= Lrs * x[s]; else acc0 -= Lrs * x[s];
+        }
+        x[r] = (acc0 + acc1) * rs[r];
+    }
+    if (lane < 12) {
+#pragma unroll
+        for (int r = 0; r < 12; r++) linv[r * 12 + lane] = x[r];
+    }
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const int* __restrict__ cptr,
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
-        const T* __restrict__ Ab, long long ltot, const double* __restrict__ g, T* Lg, double* du, int* status) {
+        const double* __restrict__ Ab, const double* __restrict__ g, double* Lg, double* du, int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* win = (T*)smem_raw;                                   // [BAND_W][BAND_W][144], row-major blocks
-    T* stage = win + BAND_W * BAND_W * 144;                  // [2][BAND_W][144]: next block row / factor column
-    T* rhs = stage + 2 * BAND_W * 144;                       // [BAND_W][12]
-    T* part = rhs + BAND_W * 12;                             // [BAND_MAX][12]
-    T* rdiag = part + BAND_MAX * 12;                         // [12] reciprocals of the diagonal factor
-    T* xs = rdiag + 12;                                      // [BAND_W][12] latest solution blocks (backward)
-    T* srec = xs + BAND_W * 12;                              // [2][12] staged reciprocals (backward)
+    double* win = (double*)smem_raw;                          // [BAND_W][BAND_W] blocks, row-major, stride BAND_BLK
+    double* stage = win + BAND_W * BAND_W * BAND_BLK;         // [2][BAND_W][144]: next block row / factor column
+    double* linv = stage + 2 * BAND_W * 144;                  // [2][144] inverse diagonal factors
+    double* rhs = linv + 2 * 144;                             // [BAND_W][12]
+    double* ybuf = rhs + BAND_W * 12;                         // [12] y_k of the current column
+    double* part = ybuf + 12;                                 // [BAND_MAX][12] (backward)
+    double* xs = part + BAND_MAX * 12;                        // [BAND_W][12] latest solution blocks (backward)
     __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
     __shared__ int ord[BAND_ORD_MAX];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid < BAND_MAX * (BAND_MAX + 1) / 2) {
         int a = 0; while ((a + 1) * (a + 2) / 2 <= tid) a++;
         tri_a[tid] = (unsigned char)a; tri_b[tid] = (unsigned char)(tid - a * (a + 1) / 2);
@@ -342,181 +411,182 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
     for (int cc = blockIdx.x; cc < ncomp; cc += gridDim.x) {
         const int N = cptr[cc + 1] - cptr[cc], wb = cbw[cc];
         for (int e = tid; e < N; e += blockDim.x) ord[e] = order[cptr[cc] + e];
-        T* L = Lg + loff[cc] * 144;                          // block L(k + d, k) at (k * BAND_W + d)
-        T* Rg = Lg + ltot * 144 + (loff[cc] / BAND_W) * 12; // reciprocal diagonal of L(k, k) at k * 12
-        const T* A = Ab + loff[cc] * 144;                    // block A(i, i - d) at (i * BAND_W + d)
+        double* L = Lg + loff[cc] * 144;                      // Linv_k at (k BAND_W), L(k + d, k) at (k BAND_W + d)
+        const double* A = Ab + loff[cc] * 144;                // block A(i, i - d) at (i BAND_W + d)
         __syncthreads();
-        auto slot = [&](int i, int j) { return win + ((i % BAND_W) * BAND_W + (j % BAND_W)) * 144; };
-        // window rows 0..min(wb, N - 1) and their right-hand sides
+        auto slot = [&](int i, int j) { return win + ((i % BAND_W) * BAND_W + (j % BAND_W)) * BAND_BLK; };
+        // window rows 0..min(wb, N - 1), their right-hand sides, and block
+        // row wb + 1 fetched ahead into its staging buffer
         const int r0 = min(wb, N - 1);
         for (int e = tid; e < (r0 + 1) * BAND_W * 144; e += blockDim.x) {
-            int i = e / (BAND_W * 144), d = (e / 144) % BAND_W;
-            if (d <= i) slot(i, i - d)[e % 144] = A[(long)e];
+            int i = e / (BAND_W * 144), d = (e / 144) % BAND_W, q = e % 144;
+            if (d <= i) slot(i, i - d)[(q / 12) * BAND_BLK + q % 12] = A[(long)e];
         }
-        for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = (T)g[12L * ord[e / 12] + e % 12];
+        for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = g[12L * ord[e / 12] + e % 12];
+        if (wb + 1 < N) {
+            double* dst = stage + ((wb + 1) & 1) * BAND_W * 144;
+            const double* src = A + (long)(wb + 1) * BAND_W * 144;
+            for (int e = tid; e < (wb + 1) * 144; e += blockDim.x) dst[(wb - e / 144) * 144 + e % 144] = src[e];
+        }
+        __syncthreads();
+        if (warp == 0) band_factor_inverse(slot(0, 0), linv, status);
         __syncthreads();
         for (int k = 0; k < N; k++) {
             const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
-            T* D = slot(k, k);
-            T* yk = rhs + (k % BAND_W) * 12;
-            if (warp == 0) {
-                // D = L_kk L_kk^T in registers: lane r < 12 holds row r; the
-                // pivot and its reciprocal square root are computed by every
-                // lane from a broadcast, so the 12 columns need no barrier
-                T a[12];
+            const double* Li = linv + (k & 1) * 144;
+            // ---- phase 1: panel L_ik = A_ik Linv_k^T (two lanes per block
+            // row: each loads the whole row, then writes six entries), and y_k
+            if (warp < 6) {
+                const int q = tid >> 1, half = tid & 1;
+                const bool act = q < 12 * nk;
+                double v[12];
+                double* R = act ? slot(k + 1 + q / 12, k) + (q % 12) * BAND_BLK : nullptr;
+                if (act) {
 #pragma unroll
-                for (int c2 = 0; c2 < 12; c2++) a[c2] = lane < 12 ? D[lane * 12 + c2] : (T)0;
-                T rs[12];
+                    for (int s = 0; s < 12; s++) v[s] = R[s];
+                }
+                __syncwarp();
+                if (act) {
 #pragma unroll
-                for (int j = 0; j < 12; j++) {
-                    T d = __shfl_sync(0xffffffffu, a[j], j);
-                    if (!(d > (T)0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + (T)1e-30; }
-                    T r = rsqrt_nr(d);
-                    rs[j] = r;
-                    T l = a[j] * r;                          // L[lane][j] for lane > j
-                    if (lane == j) a[j] = d * r;
-                    if (lane > j) a[j] = l;
-                    // full-range inner loop: every index static, so a[] stays in registers
+                    for (int c6 = 0; c6 < 6; c6++) {
+                        const int c = half * 6 + c6;
+                        double acc = 0.0;
 #pragma unroll
-                    for (int c2 = 0; c2 < 12; c2++) {
-                        T lc = __shfl_sync(0xffffffffu, l, c2);   // L[c2][j] for c2 > j
-                        if (c2 > j && lane > j) a[c2] -= l * lc;
+                        for (int s = 0; s < 12; s++) if (s <= c) acc += v[s] * Li[c * 12 + s];
+                        R[c] = acc;
                     }
                 }
-                if (lane < 12) {
+            } else if (warp == 6 && lane < 12) {
+                const double* rk = rhs + (k % BAND_W) * 12;
+                double y = 0.0;
 #pragma unroll
-                    for (int c2 = 0; c2 < 12; c2++) D[lane * 12 + c2] = c2 <= lane ? a[c2] : (T)0;
+                for (int s = 0; s < 12; s++) if (s <= lane) y += Li[lane * 12 + s] * rk[s];
+                ybuf[lane] = y;
+                du[12L * ord[k] + lane] = y;
+            }
+            __syncthreads();
+            // ---- phase 2
+            if (warp == 0) {
+                if (k + 1 < N) {
+                    // A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T (lower triangle), then factor and invert
+                    double* D = slot(k + 1, k + 1);
+                    const double* Lr = slot(k + 1, k);
+                    for (int e = lane; e < 78; e += 32) {
+                        int r = 0; while ((r + 1) * (r + 2) / 2 <= e) r++;
+                        const int c = e - r * (r + 1) / 2;
+                        double acc = 0.0;
+#pragma unroll
+                        for (int s = 0; s < 12; s++) acc += Lr[r * BAND_BLK + s] * Lr[c * BAND_BLK + s];
+                        D[r * BAND_BLK + c] -= acc;
+                    }
+                    __syncwarp();
+                    band_factor_inverse(D, linv + ((k + 1) & 1) * 144, status);
                 }
-#pragma unroll
-                for (int j = 0; j < 12; j++) if (lane == j) { rdiag[j] = rs[j]; Rg[(long)k * 12 + j] = rs[j]; }
-                // y_k = L_kk^-1 rhs_k
-                T v = lane < 12 ? yk[lane] : (T)0;
-#pragma unroll
-                for (int t = 0; t < 12; t++) {
-                    T yt = __shfl_sync(0xffffffffu, v, t) * rs[t];
-                    if (lane == t) v = yt;
-                    if (lane > t && lane < 12) v -= a[t] * yt;
-                }
-                if (lane < 12) { yk[lane] = v; du[12L * ord[k] + lane] = (double)v; }
             } else {
-                // meanwhile: block row k + wb (fetched during the previous column)
-                // enters the window, and block row k + 1 + wb is fetched
                 const int t1 = tid - 32, n1 = blockDim.x - 32;
-                if (k >= 1 && k + wb < N) {
-                    const T* src = stage + (k & 1) * BAND_W * 144;
-                    for (int e = t1; e < (wb + 1) * 144; e += n1) slot(k + wb, k + e / 144)[e % 144] = src[e];
-                    if (t1 < 12) rhs[((k + wb) % BAND_W) * 12 + t1] = (T)g[12L * ord[k + wb] + t1];
+                // A_ij -= L_ik L_jk^T over the window in 3 x 4 tiles (12 per
+                // block pair); pair 0, (k+1, k+1), is warp 0's
+                const int npair = nk * (nk + 1) / 2;
+                for (int e = t1 + 12; e < npair * 12; e += n1) {
+                    int p = e / 12, tile = e % 12;
+                    int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
+                    int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
+                    const double* Lia = slot(i, k) + r0t * BAND_BLK;
+                    const double* Ljb = slot(j, k) + c0t * BAND_BLK;
+                    double acc[3][4] = {};
+#pragma unroll
+                    for (int s = 0; s < 12; s++) {
+                        double li[3], lj[4];
+#pragma unroll
+                        for (int a2 = 0; a2 < 3; a2++) li[a2] = Lia[a2 * BAND_BLK + s];
+#pragma unroll
+                        for (int b2 = 0; b2 < 4; b2++) lj[b2] = Ljb[b2 * BAND_BLK + s];
+#pragma unroll
+                        for (int a2 = 0; a2 < 3; a2++)
+#pragma unroll
+                            for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
+                    }
+                    double* Aij = slot(i, j);
+#pragma unroll
+                    for (int a2 = 0; a2 < 3; a2++)
+#pragma unroll
+                        for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * BAND_BLK + c0t + b2] -= acc[a2][b2];
                 }
-                if (k + 1 + wb < N) {
-                    // row k + 1 + wb: block j = k + 1 + q is A(., . - d) with d = wb - q
-                    T* dst = stage + ((k + 1) & 1) * BAND_W * 144;
-                    const T* src = A + (long)(k + 1 + wb) * BAND_W * 144;
+                // rhs_i -= L_ik y_k
+                for (int t = t1; t < 12 * nk; t += n1) {
+                    int i = k + 1 + t / 12, r = t % 12;
+                    const double* R = slot(i, k) + r * BAND_BLK;
+                    double acc = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 12; c++) acc += R[c] * ybuf[c];
+                    rhs[(i % BAND_W) * 12 + r] -= acc;
+                }
+                // factor column k to global: Linv_k, then L(k + d, k)
+                for (int e = t1; e < (nk + 1) * 144; e += n1) {
+                    int d = e / 144, q = e % 144;
+                    L[((long)k * BAND_W + d) * 144 + q] = d == 0 ? Li[q] : slot(k + d, k)[(q / 12) * BAND_BLK + q % 12];
+                }
+                // block row k + 1 + wb enters the window (staged during the
+                // previous column), and row k + 2 + wb is fetched
+                const int m1 = k + 1 + wb, m2 = k + 2 + wb;
+                if (m1 < N) {
+                    const double* src = stage + (m1 & 1) * BAND_W * 144;
+                    for (int e = t1; e < (wb + 1) * 144; e += n1) {
+                        int q = e / 144, x = e % 144;             // block q: column k + 1 + q
+                        slot(m1, k + 1 + q)[(x / 12) * BAND_BLK + x % 12] = src[e];
+                    }
+                    if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = g[12L * ord[m1] + t1];
+                }
+                if (m2 < N) {
+                    // block d of the stored row is A(m2, m2 - d): column k + 2 + (wb - d)
+                    double* dst = stage + (m2 & 1) * BAND_W * 144;
+                    const double* src = A + (long)m2 * BAND_W * 144;
                     for (int e = t1; e < (wb + 1) * 144; e += n1) dst[(wb - e / 144) * 144 + e % 144] = src[e];
                 }
             }
             __syncthreads();
-            // panel: L_ik = A_ik L_kk^-T, one thread per block row
-            for (int t = tid; t < 12 * nk; t += blockDim.x) {
-                int i = k + 1 + t / 12, r = t % 12;
-                T* R = slot(i, k) + r * 12;
-                T x[12];
-#pragma unroll
-                for (int j = 0; j < 12; j++) x[j] = R[j];
-#pragma unroll
-                for (int j = 0; j < 12; j++) {
-                    T a = x[j];
-#pragma unroll
-                    for (int s = 0; s < j; s++) a -= x[s] * D[j * 12 + s];
-                    x[j] = a * rdiag[j];
-                }
-#pragma unroll
-                for (int j = 0; j < 12; j++) R[j] = x[j];
-            }
-            __syncthreads();
-            // factor column to global; rhs_i -= L_ik y_k; window update A_ij -= L_ik L_jk^T
-            for (int e = tid; e < (nk + 1) * 144; e += blockDim.x) {
-                int d = e / 144;
-                L[((long)k * BAND_W + d) * 144 + e % 144] = slot(k + d, k)[e % 144];
-            }
-            for (int t = tid; t < 12 * nk; t += blockDim.x) {
-                int i = k + 1 + t / 12, r = t % 12;
-                const T* R = slot(i, k) + r * 12;
-                T acc = 0;
-#pragma unroll
-                for (int c2 = 0; c2 < 12; c2++) acc += R[c2] * yk[c2];
-                rhs[(i % BAND_W) * 12 + r] -= acc;
-            }
-            // A_ij -= L_ik L_jk^T in 3 x 4 tiles (12 per block pair)
-            const int npair = nk * (nk + 1) / 2;
-            for (int e = tid; e < npair * 12; e += blockDim.x) {
-                int p = e / 12, tile = e % 12;
-                int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
-                int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
-                const T* Li = slot(i, k) + r0t * 12;
-                const T* Lj = slot(j, k) + c0t * 12;
-                T acc[3][4] = {};
-#pragma unroll
-                for (int s = 0; s < 12; s++) {
-                    T li[3], lj[4];
-#pragma unroll
-                    for (int a2 = 0; a2 < 3; a2++) li[a2] = Li[a2 * 12 + s];
-#pragma unroll
-                    for (int b2 = 0; b2 < 4; b2++) lj[b2] = Lj[b2 * 12 + s];
-#pragma unroll
-                    for (int a2 = 0; a2 < 3; a2++)
-#pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
-                }
-                T* Aij = slot(i, j);
-#pragma unroll
-                for (int a2 = 0; a2 < 3; a2++)
-#pragma unroll
-                    for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
-            }
-            __syncthreads();
         }
-        // backward: L^T du = y (y in du); the factor column of k is staged in
-        // shared memory while the previous one is solved
+        // backward: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}), y_k in du;
+        // the factor column of k is staged in shared memory while the
+        // previous one is solved
         {
             const int k0 = N - 1;
             for (int e = tid; e < 144; e += blockDim.x) stage[(k0 & 1) * BAND_W * 144 + e] = L[(long)k0 * BAND_W * 144 + e];
-            if (tid < 12) srec[(k0 & 1) * 12 + tid] = Rg[(long)k0 * 12 + tid];
         }
         __syncthreads();
         for (int k = N - 1; k >= 0; k--) {
             const int nk = min(wb, N - 1 - k);
-            const T* col = stage + (k & 1) * BAND_W * 144;
+            const double* col = stage + (k & 1) * BAND_W * 144;
             for (int t = tid; t < 12 * nk; t += blockDim.x) {
                 int d = 1 + t / 12, r = t % 12;              // block L(k + d, k), column r
-                const T* B = col + d * 144;
-                const T* xi = xs + ((k + d) % BAND_W) * 12;
-                T acc = 0;
+                const double* B = col + d * 144;
+                const double* xi = xs + ((k + d) % BAND_W) * 12;
+                double acc = 0.0;
 #pragma unroll
-                for (int c2 = 0; c2 < 12; c2++) acc += B[c2 * 12 + r] * xi[c2];
+                for (int c = 0; c < 12; c++) acc += B[c * 12 + r] * xi[c];
                 part[(d - 1) * 12 + r] = acc;
             }
             if (k > 0 && tid >= 128) {                        // stage column k - 1
                 const int nk1 = min(wb, N - k);
-                T* dst = stage + ((k - 1) & 1) * BAND_W * 144;
+                double* dst = stage + ((k - 1) & 1) * BAND_W * 144;
                 for (int e = tid - 128; e < (nk1 + 1) * 144; e += blockDim.x - 128)
                     dst[e] = L[(long)(k - 1) * BAND_W * 144 + e];
-                if (tid - 128 < 12) srec[((k - 1) & 1) * 12 + tid - 128] = Rg[(long)(k - 1) * 12 + tid - 128];
             }
             __syncthreads();
             if (warp == 0) {
-                T v = 0;
+                double t = 0.0;
                 if (lane < 12) {
-                    v = (T)du[12L * ord[k] + lane];
-                    for (int d = 0; d < nk; d++) v -= part[d * 12 + lane];
+                    t = du[12L * ord[k] + lane];
+                    for (int d = 0; d < nk; d++) t -= part[d * 12 + lane];
                 }
-                const T* rl = srec + (k & 1) * 12;
+                // x_k[lane] = sum_{c >= lane} Linv[c][lane] t_c
+                double x = 0.0;
 #pragma unroll
-                for (int t = 11; t >= 0; t--) {
-                    T xt = __shfl_sync(0xffffffffu, v, t) * rl[t];
-                    if (lane == t) v = xt;
-                    if (lane < t) v -= col[t * 12 + lane] * xt;
+                for (int c = 0; c < 12; c++) {
+                    double tc = __shfl_sync(0xffffffffu, t, c);
+                    if (lane < 12 && c >= lane) x += col[c * 12 + lane] * tc;
                 }
-                if (lane < 12) { du[12L * ord[k] + lane] = (double)v; xs[(k % BAND_W) * 12 + lane] = v; }
+                if (lane < 12) { du[12L * ord[k] + lane] = x; xs[(k % BAND_W) * 12 + lane] = x; }
             }
             __syncthreads();
         }
@@ -539,7 +609,7 @@ struct DenseState {
     std::vector<int> done, parent, size, root, bmap, fill;
     std::vector<int> adj_ptr, adj, pos, deg, members, mptr, bfs;
     bool smem_set[2] = {false, false};
-    bool band_smem_set[2] = {false, false};
+    bool band_smem_set = false;
 };
 static DenseState* ds_of(Engine* E) { return reinterpret_cast<DenseState*>(E->dense_state); }
 
@@ -647,8 +717,9 @@ static cusolverStatus_t lu_solve(DenseState* D, int n, T* A, T* x, T* work, int*
 template <class T>
 static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     *fallback = 0;
-    int rc = dense_init(E);
+    int rc = eng_asm_wait(E);
     if (rc) return rc;
+    if ((rc = dense_init(E))) return rc;
     DenseState* D = ds_of(E);
     cudaStream_t st = E->stream;
     const int* ndone = E->sci + SI_DONE * E->ns;
@@ -748,12 +819,11 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     for (int b = 0; b < nb; b++) {
         int r = find(b), sz = D->size[r];
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
-        // FP32 roundings of a stiff projected Hessian can make it indefinite:
-        // the band Cholesky (no pivoting, no fallback) runs in FP64 mode only
-        // a single CTA walks the band sequentially, so cuSOLVER (all SMs) is
-        // faster for a component above BAND_PREFER_MAX bodies while few such
-        // components exist
-        if (D->root[r] == -1 && projected && !E->mixed &&
+        // the band Cholesky factors in FP64 in both precision modes; a single
+        // CTA walks the band sequentially, so cuSOLVER (all SMs) is faster for
+        // a component above BAND_PREFER_MAX bodies while few such components
+        // exist
+        if (D->root[r] == -1 && projected &&
             (sz <= BAND_PREFER_MAX || (int)large_n.size() >= MAX_LARGE_COMPONENTS / 2)) {
             int bw = rcm(r, ord);
             if (bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
@@ -827,7 +897,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         const int* d_bcptr = d_sbody + small_bodies;
         const int* d_bbw = d_bcptr + nband + 1;
         const int* d_bord = d_bbw + nband;
-        size_t need = ((size_t)lblocks * 144 + 12 * band_order.size()) * sizeof(T);
+        size_t need = (size_t)lblocks * 144 * sizeof(double);
         if (need > D->Lg_bytes) {
             if (D->Lg) cudaFree(D->Lg);
             if (D->Ab) cudaFree(D->Ab);
@@ -839,25 +909,27 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
             }
         }
         CUDA_TRY(cudaMemcpyAsync(D->loff_d, D->loff_h, sizeof(long long) * nband, cudaMemcpyHostToDevice, st));
-        const size_t smem = ((size_t)BAND_W * BAND_W * 144 + 2 * BAND_W * 144 + BAND_W * 12 + BAND_MAX * 12 + 12 +
-                             BAND_W * 12 + 24) * sizeof(T);
-        if (!D->band_smem_set[sizeof(T) == 8]) {
-            CUDA_TRY(cudaFuncSetAttribute(k_band_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            D->band_smem_set[sizeof(T) == 8] = true;
+        // window, staging, inverse diagonal factors, right-hand sides, y_k,
+        // backward partial sums and solution blocks
+        const size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 +
+                             BAND_MAX * 12 + BAND_W * 12) * sizeof(double);
+        if (!D->band_smem_set) {
+            CUDA_TRY(cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            D->band_smem_set = true;
         }
         const int* d_pcomp = d_bord + band_order.size();
         const int npos = (int)band_order.size();
         k_band_gather<T><<<grid_for(32L * npos * BAND_W), 256, 0, st>>>(npos, d_pcomp, d_bcptr, d_bord, d_bbw, D->loff_d,
-                                                                       E->row_ptr, E->bcol, (const T*)E->vals, (T*)D->Ab);
+                                                                       E->row_ptr, E->bcol, (const T*)E->vals, (double*)D->Ab);
         E->launches++;
         int ph = phase_begin(E, PH_BAND);
-        k_band_solve<T><<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, (const T*)D->Ab,
-                                                           lblocks, E->g, (T*)D->Lg, E->du, D->info);
+        k_band_solve<<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, (const double*)D->Ab,
+                                                        E->g, (double*)D->Lg, E->du, D->info);
         // per component: band blocks read, factor written and read back,
         // g read, y and du written and read
         double bytes = 0;
         for (int c = 0; c < nband; c++)
-            bytes += (band_cptr[c + 1] - band_cptr[c]) * ((band_bw[c] + 1) * 144.0 * sizeof(T) * 3 + 96.0 * 4);
+            bytes += (band_cptr[c + 1] - band_cptr[c]) * ((band_bw[c] + 1) * 144.0 * sizeof(double) * 3 + 96.0 * 4);
         phase_end(E, ph, bytes);
         E->launches++;
     }

@@ -156,6 +156,10 @@ struct Engine {
     unsigned long long* keys = nullptr; unsigned long long* keys_s = nullptr; unsigned long long* ukeys = nullptr;
     int blk_cap = 0;
     int nnzb_host = 0;             // block count of the last assembly (host copy)
+    long long dense_blocks = 0;    // sum over scenes of n_bodies^2: no assembly has more blocks
+    // the assembly's counters and block keys travel to the host behind
+    // ev_asm while its kernels keep running; eng_asm_wait collects them
+    cudaEvent_t ev_asm = nullptr; bool asm_pending = false; bool asm_direct = false;
     int* row_ptr = nullptr; int* bcol = nullptr;
     void* vals = nullptr;          // double or float [blk_cap*144]
     void* dinv = nullptr;          // [nb*144]
@@ -297,6 +301,7 @@ int eng_ccd(Engine* E, const double* dq, double sign); // per-scene toi into scd
 int eng_step(Engine* E, int n_steps, AbdStepStats* stats);
 int eng_intersections(Engine* E, int* count);
 int eng_sync_counters(Engine* E);
+int eng_asm_wait(Engine* E);                           // counters and block keys of the last assembly on the host
 int eng_grid_build(Engine* E, Grid& G);
 GridView eng_view(const Grid& G);
 int eng_swept(Engine* E, const double* dq, double sign, const int* done);

@@ -300,6 +300,8 @@ __global__ void k_copy_out(int n, const T* __restrict__ x, double* du) { GS_LOOP
 
 template <class T>
 static int solve_t(Engine* E, int* iters) {
+    int rc0 = eng_asm_wait(E);
+    if (rc0) return rc0;
     cudaStream_t st = E->stream;
     int ns = E->ns, nb = E->nb;
     T* kv[10];
