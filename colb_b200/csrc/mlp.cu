@@ -13,9 +13,11 @@
 // the next layer's BF16 operand.  Every wait is bounded and reports through
 // an error flag; tensor memory is freed on every path.
 //
-// Training: FP32 master weights, Adam, plain SIMT kernels over a mini-batch
-// (forward with BF16-rounded weights and activations like inference, MSE
-// loss, backward with straight-through rounding).
+// Training: FP32 master weights, Adam; every GEMM of the forward and backward
+// pass (Z = H W^T, dW = dZ^T H, dH = dZ W) on the tensor cores (tcgen05,
+// BF16 operands, FP32 accumulation in tensor memory), the forward with
+// BF16-rounded weights and activations like inference, MSE loss, backward
+// with straight-through rounding.
 #include "engine.cuh"
 #include <cuda_bf16.h>
 
@@ -260,42 +262,102 @@ __global__ void k_mlp_pack(const float* __restrict__ P, __nv_bfloat16* pack, flo
 }
 
 // ------------------------------------------------------------------ training kernels
-// C[m][n] = sum_k A(m,k) B(k,n) (+ bias[n]); A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn]
-__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const float* __restrict__ A, long sam, long sak,
-                                             const float* __restrict__ B, long sbk, long sbn, float* __restrict__ C,
-                                             int ldc, const float* __restrict__ bias) {
-    __shared__ float As[16][65], Bs[16][65];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        for (int e = threadIdx.x; e < 1024; e += 256) {
-            int kk = e / 64, mm = e % 64;
-            int m = m0 + mm, k = k0 + kk;
-            As[kk][mm] = (m < M && k < K) ? A[m * sam + k * sak] : 0.0f;
-            int nn = mm, nI = n0 + nn;
-            Bs[kk][nn] = (nI < N && k < K) ? B[k * sbk + nI * sbn] : 0.0f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < 16; kk++) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) { a[i] = As[kk][ty * 4 + i]; b[i] = Bs[kk][tx * 4 + i]; }
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
-        }
-        __syncthreads();
+// Training GEMMs on the tensor cores:
+//   C[m][n] = sum_k A(m,k) B(k,n) (+ bias[n]),
+//   A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn]
+// (the strides express the transposes of the backward pass).  One CTA of 4
+// warps computes a 128 x 64 tile of C: the operands are staged 64 k at a time
+// into shared memory, rounded to BF16, in the UMMA canonical K-major layout
+// (8x8 core matrices, no swizzle; the staging writes any transpose into that
+// layout), one elected thread issues tcgen05.mma (kind::f16, M = 128,
+// N = 64, K = 16 per instruction) into a 64-column FP32 accumulator in tensor
+// memory, and the warps read their 32 lanes back with tcgen05.ld.  Waits are
+// bounded and report through *err; tensor memory is freed on every path.
+constexpr int TG_M = 128, TG_N = 64, TG_K = 64, TG_THR = 128;
+constexpr int TG_SA = 0, TG_SB = TG_SA + TG_M * TG_K * 2, TG_BAR = TG_SB + TG_N * TG_K * 2, TG_TM = TG_BAR + 8,
+              TG_TOT = TG_TM + 8;
+__global__ void __launch_bounds__(TG_THR) k_tc_gemm(int M, int N, int K, const float* __restrict__ A, long sam, long sak,
+                                                    const float* __restrict__ B, long sbk, long sbn, float* __restrict__ C,
+                                                    int ldc, const float* __restrict__ bias, int* err) {
+    __shared__ __align__(1024) uint8_t smem[TG_TOT];
+    __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(smem + TG_SA);
+    __nv_bfloat16* sB = reinterpret_cast<__nv_bfloat16*>(smem + TG_SB);
+    const uint32_t aA = smem_u32(smem + TG_SA), aB = smem_u32(smem + TG_SB), bar = smem_u32(smem + TG_BAR);
+    uint32_t* tm_holder = reinterpret_cast<uint32_t*>(smem + TG_TM);
+    __shared__ int status;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TG_M, n0 = blockIdx.x * TG_N;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tm_holder)), "r"(TG_N) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    if (tid == 0) {
+        status = 0;
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tm_holder;
+    int chunk = 0;
+    for (int k0 = 0; k0 < K; k0 += TG_K, chunk++) {
+        // operands of this k range, zero outside the matrices
+        for (int e = tid; e < (TG_M + TG_N) * (TG_K / 8); e += TG_THR) {
+            const bool isA = e < TG_M * (TG_K / 8);
+            const int f = isA ? e : e - TG_M * (TG_K / 8);
+            const int r = f / (TG_K / 8), kg = (f % (TG_K / 8)) * 8;
+            __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            int m = m0 + ty * 4 + i, nI = n0 + tx * 4 + j;
-            if (m < M && nI < N) C[(long)m * ldc + nI] = acc[i][j] + (bias ? bias[nI] : 0.0f);
+            for (int j = 0; j < 8; j++) {
+                const int k = k0 + kg + j;
+                float x = 0.0f;
+                if (isA) { const int m = m0 + r; if (m < M && k < K) x = A[(long)m * sam + (long)k * sak]; }
+                else { const int n = n0 + r; if (n < N && k < K) x = B[(long)k * sbk + (long)n * sbn]; }
+                v[j] = __float2bfloat16_rn(x);
+            }
+            __nv_bfloat16* dst = (isA ? sA : sB) + canon(r, kg, TG_K);
+            *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
         }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t id = idesc(TG_N), sbo = (uint32_t)TG_K * 16;
+#pragma unroll
+            for (int kk = 0; kk < TG_K / 16; kk++)
+                mma_bf16(tmem, sdesc(aA + kk * 256, 128, sbo), sdesc(aB + kk * 256, 128, sbo), id, (chunk > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(bar);
+            // the next chunk overwrites the operands: wait for these MMAs
+            if (!mbar_wait(bar, chunk & 1)) { status = 1; atomicExch(err, 1); }
+        }
+        __syncthreads();
+        if (status) break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!status && K > 0) {
+        const int m = m0 + warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < TG_N; c0 += 32) {
+            float v[32];
+            tmem_ld32(trow + c0, v);
+            if (m < M) {
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const int n = n0 + c0 + j;
+                    if (n < N) C[(long)m * ldc + n] = v[j] + (bias ? bias[n] : 0.0f);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TG_N) : "memory");
+    }
 }
 __global__ void k_round(long n, const float* __restrict__ a, float* b) { GS_LOOP(i, n) b[i] = bf16r(a[i]); }
 __global__ void k_gelu_round(long n, const float* __restrict__ z, float* h) { GS_LOOP(i, n) h[i] = bf16r(gelu(z[i])); }
@@ -497,6 +559,7 @@ struct AbdTrainer {
     float *Xb = nullptr, *Tb = nullptr, *Z[3] = {}, *H[3] = {}, *Y = nullptr, *dY = nullptr, *dA = nullptr, *dB = nullptr;
     int* idx = nullptr;
     float* loss = nullptr;
+    int* dflag = nullptr;              // set by a tensor-core GEMM whose wait gave up
     std::string err;
 };
 
@@ -524,7 +587,7 @@ static bool tr_reserve(AbdTrainer* T, int b) {
     if (ok) T->bcap = b;
     return ok;
 }
-static dim3 gemm_grid(int M, int N) { return dim3((N + 63) / 64, (M + 63) / 64); }
+static dim3 gemm_grid(int M, int N) { return dim3((N + TG_N - 1) / TG_N, (M + TG_M - 1) / TG_M); }
 
 // loss and gradient (into T->G) of the batch in Xb / Tb (b rows)
 static void tr_forward_backward(AbdTrainer* T, int b) {
@@ -537,7 +600,8 @@ static void tr_forward_backward(AbdTrainer* T, int b) {
     // forward: Z = Hin W^T + b
     for (int l = 0; l < 4; l++) {
         float* Zl = l < 3 ? T->Z[l] : T->Y;
-        k_gemm<<<gemm_grid(b, out[l]), 256, 0, s>>>(b, out[l], in[l], Hin[l], in[l], 1, W[l], 1, in[l], Zl, out[l], Bs[l]);
+        k_tc_gemm<<<gemm_grid(b, out[l]), TG_THR, 0, s>>>(b, out[l], in[l], Hin[l], in[l], 1, W[l], 1, in[l], Zl, out[l], Bs[l],
+                                                         T->dflag);
         if (l < 3) k_gelu_round<<<grid_for((long)b * MH), 256, 0, s>>>((long)b * MH, Zl, T->H[l]);
     }
     cudaMemsetAsync(T->loss, 0, sizeof(float), s);
@@ -545,12 +609,13 @@ static void tr_forward_backward(AbdTrainer* T, int b) {
     // backward: dW = dZ^T Hin, db = colsum dZ, dHin = dZ W
     float* dZ = T->dY;
     for (int l = 3; l >= 0; l--) {
-        k_gemm<<<gemm_grid(out[l], in[l]), 256, 0, s>>>(out[l], in[l], b, dZ, 1, out[l], Hin[l], in[l], 1,
-                                                        T->G + gW[l], in[l], nullptr);
+        k_tc_gemm<<<gemm_grid(out[l], in[l]), TG_THR, 0, s>>>(out[l], in[l], b, dZ, 1, out[l], Hin[l], in[l], 1,
+                                                              T->G + gW[l], in[l], nullptr, T->dflag);
         k_colsum<<<grid_for(out[l]), 256, 0, s>>>(b, out[l], dZ, T->G + gB[l]);
         if (l > 0) {
             float* dH = (dZ == T->dA) ? T->dB : T->dA;
-            k_gemm<<<gemm_grid(b, in[l]), 256, 0, s>>>(b, in[l], out[l], dZ, out[l], 1, W[l], in[l], 1, dH, in[l], nullptr);
+            k_tc_gemm<<<gemm_grid(b, in[l]), TG_THR, 0, s>>>(b, in[l], out[l], dZ, out[l], 1, W[l], in[l], 1, dH, in[l], nullptr,
+                                                             T->dflag);
             k_gelu_back<<<grid_for((long)b * MH), 256, 0, s>>>((long)b * MH, T->Z[l - 1], dH);
             dZ = dH;
         }
@@ -570,7 +635,8 @@ extern "C" int abd_trainer_create(int32_t device, const float* params, AbdTraine
     }
     size_t nb = sizeof(float) * NPARAM;
     if (cudaMalloc(&T->P, nb) != cudaSuccess || cudaMalloc(&T->Pq, nb) != cudaSuccess || cudaMalloc(&T->G, nb) != cudaSuccess ||
-        cudaMalloc(&T->m, nb) != cudaSuccess || cudaMalloc(&T->v, nb) != cudaSuccess || cudaMalloc(&T->loss, sizeof(float)) != cudaSuccess) {
+        cudaMalloc(&T->m, nb) != cudaSuccess || cudaMalloc(&T->v, nb) != cudaSuccess || cudaMalloc(&T->loss, sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&T->dflag, sizeof(int)) != cudaSuccess) {
         *out = T;
         T->err = "cudaMalloc trainer";
         return ABD_ERR_CUDA;
@@ -579,6 +645,7 @@ extern "C" int abd_trainer_create(int32_t device, const float* params, AbdTraine
     TR_TRY(cudaMemcpyAsync(T->P, params, nb, cudaMemcpyHostToDevice, T->s));
     TR_TRY(cudaMemsetAsync(T->m, 0, nb, T->s));
     TR_TRY(cudaMemsetAsync(T->v, 0, nb, T->s));
+    TR_TRY(cudaMemsetAsync(T->dflag, 0, sizeof(int), T->s));
     k_round<<<grid_for(NPARAM), 256, 0, T->s>>>(NPARAM, T->P, T->Pq);
     TR_TRY(cudaStreamSynchronize(T->s));
     return ABD_OK;
@@ -590,6 +657,7 @@ extern "C" int abd_trainer_destroy(AbdTrainer* T) {
     tr_free_batch(T);
     float* ps[] = {T->P, T->Pq, T->G, T->m, T->v, T->X, T->T, T->loss};
     for (float* p : ps) if (p) cudaFree(p);
+    if (T->dflag) cudaFree(T->dflag);
     if (T->s) cudaStreamDestroy(T->s);
     delete T;
     return ABD_OK;
@@ -638,8 +706,11 @@ extern "C" int abd_trainer_epoch(AbdTrainer* T, const int32_t* order, int32_t n,
     }
     std::vector<float> hl(nbat);
     TR_TRY(cudaMemcpyAsync(hl.data(), dl, sizeof(float) * nbat, cudaMemcpyDeviceToHost, T->s));
+    int flag = 0;
+    TR_TRY(cudaMemcpyAsync(&flag, T->dflag, sizeof(int), cudaMemcpyDeviceToHost, T->s));
     TR_TRY(cudaStreamSynchronize(T->s));
     cudaFree(dl); cudaFree(didx);
+    if (flag) { T->err = "tensor-core GEMM: an mbarrier wait gave up"; return ABD_ERR_CUDA; }
     double s = 0;
     for (float v : hl) s += v;
     if (mean_loss) *mean_loss = (float)(s / nbat);
@@ -658,8 +729,11 @@ extern "C" int abd_trainer_grad(AbdTrainer* T, const float* x, const float* y, i
     tr_forward_backward(T, n);
     TR_TRY(cudaMemcpyAsync(grad, T->G, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost, T->s));
     float l = 0;
+    int flag = 0;
     TR_TRY(cudaMemcpyAsync(&l, T->loss, sizeof(float), cudaMemcpyDeviceToHost, T->s));
+    TR_TRY(cudaMemcpyAsync(&flag, T->dflag, sizeof(int), cudaMemcpyDeviceToHost, T->s));
     TR_TRY(cudaStreamSynchronize(T->s));
+    if (flag) { T->err = "tensor-core GEMM: an mbarrier wait gave up"; return ABD_ERR_CUDA; }
     if (loss) *loss = l;
     return ABD_OK;
 }

@@ -105,9 +105,13 @@ def loss_grad(p, xn, yn, rounding=True):
     grads = [None] * 4
     for l in range(3, -1, -1):
         W, _ = layers[l]
-        grads[l] = (dz.T @ hs[l], dz.sum(axis=0))
+        # the GPU trainer's backward GEMMs run on the tensor cores with BF16
+        # operands and FP32 sums: dW = bf16(dZ)^T H, dH = bf16(dZ) bf16(W);
+        # the bias gradient sums the FP32 dZ
+        dzr = rnd(dz)
+        grads[l] = (dzr.T @ hs[l], dz.sum(axis=0))
         if l > 0:
-            dh = dz @ rnd(W)
+            dh = dzr @ rnd(W)
             dz = (dh * gelu_grad(zs[l - 1])).astype(np.float32)
     return loss, pack(grads)
 
