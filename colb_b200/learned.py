@@ -11,8 +11,11 @@ only changes where Newton starts.
 
     python -m colb_b200.learned --out colb_b200/data/warmstart_net16.npz
 
-trains the network shipped with the package on chain-net scenes with
-seeds and shapes disjoint from the evaluation seeds.
+trains the network shipped with the package on at least 2e5 (features,
+converged increment) pairs from 16 x 16 chain nets (seeds TRAIN_SEEDS, 200
+steps each from t = 0: fall, impact and rest), then evaluates it against the
+plain start on held-out seeds (EVAL_SEEDS) and stores that evaluation in the
+model file's metadata.
 """
 import argparse
 import json
@@ -55,6 +58,52 @@ def collect(engine, steps, mass):
         X.append(f[dyn])
         Y.append(body_targets(s0, s1, prm.dt, list(prm.gravity))[dyn])
     return np.concatenate(X), np.concatenate(Y)
+
+
+def c2_scenes(seeds, vary=True):
+    """16 x 16 chain nets of the chain-net configuration (R = 1, r = 0.25,
+    corners pinned) with the given seeds; `vary` also draws the pitch in
+    [1.48, 1.49], the lift in [0.85, 0.9] and the velocity noise in
+    [1e-3, 5e-2] from the seed."""
+    out = []
+    for sd in seeds:
+        rng = np.random.default_rng(10_000 + sd)
+        kw = dict(pitch=float(rng.uniform(1.48, 1.49)), lift=float(rng.uniform(0.85, 0.9)),
+                  vel_noise=float(rng.uniform(1e-3, 5e-2))) if vary else {}
+        out.append(S.config2_chain_net(n=16, seed=int(sd), **kw))
+    return out
+
+
+def evaluate(params, norm, scenes, steps, rest_from=120, dt=1.0 / 240.0, device=0, log=None):
+    """Plain start against the learned warm start on each scene from t = 0:
+    Newton iterations and device milliseconds per step, over all steps and
+    over the steps from `rest_from` on (the resting net), with the
+    unconverged steps and intersections of both."""
+    rows = []
+    for k, sc in enumerate(scenes):
+        row = {}
+        for name, ws in (("plain", 0), ("learned", 3)):
+            e = Engine(P.config_params(dt=dt, warm_start=ws), sc, device=device)
+            if ws == 3:
+                e.set_mlp(params, norm)
+            it, ms, unconv = [], [], 0
+            for _ in range(steps):
+                rc, st = e.step(1, allow=(-6, -7))
+                it.append(st.newton_iters); ms.append(st.gpu_ms); unconv += st.unconverged
+            it, ms = np.array(it, float), np.array(ms, float)
+            row[name] = dict(iters=float(it.mean()), ms=float(ms.mean()), iters_rest=float(it[rest_from:].mean()),
+                             ms_rest=float(ms[rest_from:].mean()), unconverged=int(unconv),
+                             intersections=int(e.count_intersections()))
+            e.close()
+        row["iter_ratio"] = row["learned"]["iters"] / row["plain"]["iters"]
+        row["iter_ratio_rest"] = row["learned"]["iters_rest"] / row["plain"]["iters_rest"]
+        row["time_ratio"] = row["learned"]["ms"] / row["plain"]["ms"]
+        rows.append(row)
+        if log:
+            log(f"eval scene {k}: {json.dumps(row)}")
+    mean = lambda key: float(np.mean([r[key] for r in rows]))
+    return dict(scenes=rows, iter_ratio=mean("iter_ratio"), iter_ratio_rest=mean("iter_ratio_rest"),
+                time_ratio=mean("time_ratio"), steps=steps, rest_from=rest_from)
 
 
 def training_scenes(count, seed=0, n_range=(8, 16)):
@@ -130,26 +179,43 @@ def run_steps(engine, steps):
     return np.array(iters), np.array(ms)
 
 
+TRAIN_SEEDS = tuple(range(1000, 1004))    # chain-net seeds the network is trained on
+EVAL_SEEDS = (500, 501)                    # held out: never seen in training (the benchmark net is seed 0)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out", default=DEFAULT_MODEL)
-    ap.add_argument("--scenes", type=int, default=8)
-    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--pairs", type=int, default=200_000, help="training pairs to collect (at least)")
+    ap.add_argument("--steps", type=int, default=200, help="steps per training scene")
     ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--eval-steps", type=int, default=160)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
     t0 = time.time()
     Xs, Ys = [], []
-    for sc in training_scenes(args.scenes, args.seed):
+    seeds = []
+    for sd in TRAIN_SEEDS + tuple(range(2000, 2100)):
+        if sum(len(x) for x in Xs) >= args.pairs:
+            break
+        sc = c2_scenes([sd])[0]
         e = Engine(P.config_params(dt=1.0 / 240.0), sc)
         X, Y = collect(e, args.steps, sc["mass"])
-        Xs.append(X); Ys.append(Y)
+        Xs.append(X); Ys.append(Y); seeds.append(sd)
         e.close()
+        print(f"scene seed {sd}: {len(X)} pairs ({time.time() - t0:.1f} s)", flush=True)
     X, Y = np.concatenate(Xs), np.concatenate(Ys)
     print(f"collected {len(X)} pairs in {time.time() - t0:.1f} s", flush=True)
+    t1 = time.time()
     params, norm, losses = train(X, Y, epochs=args.epochs, seed=args.seed, log=print)
-    save(args.out, params, norm, dict(pairs=int(len(X)), epochs=args.epochs, final_loss=float(losses[-1]),
-                                     scenes=args.scenes, steps=args.steps, seed=args.seed))
+    train_s = time.time() - t1
+    ev = evaluate(params, norm, c2_scenes(EVAL_SEEDS), args.eval_steps, log=print)
+    meta = dict(pairs=int(len(X)), epochs=args.epochs, final_loss=float(losses[-1]), train_seconds=train_s,
+                train_seeds=seeds, steps=args.steps, seed=args.seed, eval_seeds=list(EVAL_SEEDS), eval=ev)
+    save(args.out, params, norm, meta)
+    print(json.dumps({k: v for k, v in meta.items() if k != "eval"}))
+    print(f"eval: iterations learned/plain {ev['iter_ratio']:.3f} (resting {ev['iter_ratio_rest']:.3f}), "
+          f"device time learned/plain {ev['time_ratio']:.3f}")
     print(f"saved {args.out} ({time.time() - t0:.1f} s)")
 
 
