@@ -286,10 +286,10 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_solve(int nsmall, const
 // The 12 dependent pivots of each diagonal block thereby run beside the
 // trailing update instead of before it.  The backward solve walks the
 // columns again: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).
-// The factorization runs in FP64 in both precision modes: a mixed-precision
-// handle gathers its FP32 blocks into FP64, because FP32 roundings of a
-// stiff projected Hessian can make a pivot non-positive and the band path
-// has no pivoting fallback.
+// FP64 mode only: the FP32 blocks of a mixed-precision handle can be
+// indefinite (roundings of a stiff, PSD-projected Hessian), and the band
+// path has no pivoting fallback, so mixed-precision components take the
+// shared-memory or cuSOLVER paths, which fall back to LU.
 constexpr int BAND_MAX = 8;
 constexpr int BAND_W = BAND_MAX + 1;
 constexpr int BAND_THREADS = 256;
@@ -338,8 +338,8 @@ __global__ void k_band_gather(int npos, const int* __restrict__ pcomp, const int
     }
 }
 
-// Warp-wide: Cholesky factor of the 12x12 SPD block D (row-major, stride
-// BAND_BLK, lower triangle read), written back into D's lower triangle, and
+// Warp-wide: Cholesky factor of the 12x12 SPD block D (row-major, lower
+// triangle read), written back into D's lower triangle, and
 // its inverse Linv = L^-1 (row-major 12x12, zeros above the diagonal).  Lane
 // r holds row r; each pivot is broadcast, its reciprocal square root computed
 // by every lane, so the 12 columns need no barrier.  A non-positive pivot
@@ -348,7 +348,7 @@ DV void band_factor_inverse(double* D, double* linv, int* status) {
     const int lane = threadIdx.x & 31;
     double a[12], rs[12];
 #pragma unroll
-    for (int c = 0; c < 12; c++) a[c] = lane < 12 ? D[lane * BAND_BLK + c] : 0.0;
+    for (int c = 0; c < 12; c++) a[c] = lane < 12 ? D[lane * 12 + c] : 0.0;
 #pragma unroll
     for (int j = 0; j < 12; j++) {
         double d = __shfl_sync(0xffffffffu, a[j], j);
@@ -367,7 +367,7 @@ DV void band_factor_inverse(double* D, double* linv, int* status) {
     }
     if (lane < 12) {
 #pragma unroll
-        for (int c = 0; c < 12; c++) if (c <= lane) D[lane * BAND_BLK + c] = a[c];
+        for (int c = 0; c < 12; c++) if (c <= lane) D[lane * 12 + c] = a[c];
     }
     __syncwarp();
     // column `lane` of L^-1 by forward substitution, L[r][s] broadcast from
@@ -378,7 +378,7 @@ DV void band_factor_inverse(double* D, double* linv, int* status) {
         double acc0 = (lane == r) ? 1.0 : 0.0, acc1 = 0.0;
 #pragma unroll
         for (int s = 0; s < r; s++) {
-            double Lrs = D[r * BAND_BLK + s];
+            double Lrs = D[r * 12 + s];
             if (s & 1) acc1 -= Lrs * x[s]; else acc0 -= Lrs * x[s];
         }
         x[r] = (acc0 + acc1) * rs[r];
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
         const double* __restrict__ Ab, const double* __restrict__ g, double* Lg, double* du, int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* win = (double*)smem_raw;                          // [BAND_W][BAND_W] blocks, row-major, stride BAND_BLK
+    double* win = (double*)smem_raw;                          // [BAND_W][BAND_W] row-major 12x12 blocks, BAND_BLK apart
     double* stage = win + BAND_W * BAND_W * BAND_BLK;         // [2][BAND_W][144]: next block row / factor column
     double* linv = stage + 2 * BAND_W * 144;                  // [2][144] inverse diagonal factors
     double* rhs = linv + 2 * 144;                             // [BAND_W][12]
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         const int r0 = min(wb, N - 1);
         for (int e = tid; e < (r0 + 1) * BAND_W * 144; e += blockDim.x) {
             int i = e / (BAND_W * 144), d = (e / 144) % BAND_W, q = e % 144;
-            if (d <= i) slot(i, i - d)[(q / 12) * BAND_BLK + q % 12] = A[(long)e];
+            if (d <= i) slot(i, i - d)[q] = A[(long)e];
         }
         for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = g[12L * ord[e / 12] + e % 12];
         if (wb + 1 < N) {
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 const int q = tid >> 1, half = tid & 1;
                 const bool act = q < 12 * nk;
                 double v[12];
-                double* R = act ? slot(k + 1 + q / 12, k) + (q % 12) * BAND_BLK : nullptr;
+                double* R = act ? slot(k + 1 + q / 12, k) + (q % 12) * 12 : nullptr;
                 if (act) {
 #pragma unroll
                     for (int s = 0; s < 12; s++) v[s] = R[s];
@@ -476,8 +476,8 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                         const int c = e - r * (r + 1) / 2;
                         double acc = 0.0;
 #pragma unroll
-                        for (int s = 0; s < 12; s++) acc += Lr[r * BAND_BLK + s] * Lr[c * BAND_BLK + s];
-                        D[r * BAND_BLK + c] -= acc;
+                        for (int s = 0; s < 12; s++) acc += Lr[r * 12 + s] * Lr[c * 12 + s];
+                        D[r * 12 + c] -= acc;
                     }
                     __syncwarp();
                     band_factor_inverse(D, linv + ((k + 1) & 1) * 144, status);
@@ -491,16 +491,16 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     int p = e / 12, tile = e % 12;
                     int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
                     int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
-                    const double* Lia = slot(i, k) + r0t * BAND_BLK;
-                    const double* Ljb = slot(j, k) + c0t * BAND_BLK;
+                    const double* Lia = slot(i, k) + r0t * 12;
+                    const double* Ljb = slot(j, k) + c0t * 12;
                     double acc[3][4] = {};
 #pragma unroll
                     for (int s = 0; s < 12; s++) {
                         double li[3], lj[4];
 #pragma unroll
-                        for (int a2 = 0; a2 < 3; a2++) li[a2] = Lia[a2 * BAND_BLK + s];
+                        for (int a2 = 0; a2 < 3; a2++) li[a2] = Lia[a2 * 12 + s];
 #pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) lj[b2] = Ljb[b2 * BAND_BLK + s];
+                        for (int b2 = 0; b2 < 4; b2++) lj[b2] = Ljb[b2 * 12 + s];
 #pragma unroll
                         for (int a2 = 0; a2 < 3; a2++)
 #pragma unroll
@@ -510,12 +510,12 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
 #pragma unroll
                     for (int a2 = 0; a2 < 3; a2++)
 #pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * BAND_BLK + c0t + b2] -= acc[a2][b2];
+                        for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
                 }
                 // rhs_i -= L_ik y_k
                 for (int t = t1; t < 12 * nk; t += n1) {
                     int i = k + 1 + t / 12, r = t % 12;
-                    const double* R = slot(i, k) + r * BAND_BLK;
+                    const double* R = slot(i, k) + r * 12;
                     double acc = 0.0;
 #pragma unroll
                     for (int c = 0; c < 12; c++) acc += R[c] * ybuf[c];
@@ -524,7 +524,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 // factor column k to global: Linv_k, then L(k + d, k)
                 for (int e = t1; e < (nk + 1) * 144; e += n1) {
                     int d = e / 144, q = e % 144;
-                    L[((long)k * BAND_W + d) * 144 + q] = d == 0 ? Li[q] : slot(k + d, k)[(q / 12) * BAND_BLK + q % 12];
+                    L[((long)k * BAND_W + d) * 144 + q] = d == 0 ? Li[q] : slot(k + d, k)[q];
                 }
                 // block row k + 1 + wb enters the window (staged during the
                 // previous column), and row k + 2 + wb is fetched
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     const double* src = stage + (m1 & 1) * BAND_W * 144;
                     for (int e = t1; e < (wb + 1) * 144; e += n1) {
                         int q = e / 144, x = e % 144;             // block q: column k + 1 + q
-                        slot(m1, k + 1 + q)[(x / 12) * BAND_BLK + x % 12] = src[e];
+                        slot(m1, k + 1 + q)[x] = src[e];
                     }
                     if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = g[12L * ord[m1] + t1];
                 }
@@ -819,11 +819,12 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     for (int b = 0; b < nb; b++) {
         int r = find(b), sz = D->size[r];
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
-        // the band Cholesky factors in FP64 in both precision modes; a single
-        // CTA walks the band sequentially, so cuSOLVER (all SMs) is faster for
-        // a component above BAND_PREFER_MAX bodies while few such components
-        // exist
-        if (D->root[r] == -1 && projected &&
+        // FP32 roundings of a stiff projected Hessian can make it indefinite:
+        // the band Cholesky (no pivoting, no fallback) runs in FP64 mode only;
+        // a single CTA walks the band sequentially, so cuSOLVER (all SMs) is
+        // faster for a component above BAND_PREFER_MAX bodies while few such
+        // components exist
+        if (D->root[r] == -1 && projected && !E->mixed &&
             (sz <= BAND_PREFER_MAX || (int)large_n.size() >= MAX_LARGE_COMPONENTS / 2)) {
             int bw = rcm(r, ord);
             if (bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
