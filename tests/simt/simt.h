@@ -1,0 +1,67 @@
+// Host-side emulation of the CUDA execution model for testing kernel source
+// on a machine without a GPU: every thread of a block runs as a std::thread,
+// __syncthreads and __syncwarp are std::barriers, __shfl_sync exchanges
+// through a per-warp array between two warp barriers, and the dynamic shared
+// memory is one host buffer.  Blocks of a grid run one after the other.  It
+// covers what the direct solver's band kernel uses; a kernel that needs
+// anything else (tensor cores, atomics on shared memory, clusters) does not
+// compile against it.
+#pragma once
+#include <barrier>
+#include <thread>
+#include <vector>
+#include <cmath>
+#include <atomic>
+#include <algorithm>
+#include <cstring>
+#include <cstdint>
+#include <cstdio>
+struct dim3 { unsigned x = 1, y = 1, z = 1; };
+inline thread_local dim3 threadIdx, blockIdx;
+inline dim3 blockDim, gridDim;
+inline std::barrier<>* g_block_bar = nullptr;
+inline std::vector<std::barrier<>*> g_warp_bar;
+inline double g_xd[64][32];
+inline unsigned char* g_dyn_smem = nullptr;
+#define __global__
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __restrict__
+#define __launch_bounds__(...)
+#define __align__(x) alignas(x)
+#define DV inline
+#define HD inline
+using std::min; using std::max;
+inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
+inline void __syncthreads() { g_block_bar->arrive_and_wait(); }
+inline void __syncwarp(unsigned = 0xffffffffu) { g_warp_bar[threadIdx.x / 32]->arrive_and_wait(); }
+inline double __shfl_sync(unsigned, double v, int src) {
+    int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    g_xd[w][l] = v;
+    g_warp_bar[w]->arrive_and_wait();
+    double r = g_xd[w][src & 31];
+    g_warp_bar[w]->arrive_and_wait();
+    return r;
+}
+inline float __shfl_sync(unsigned m, float v, int src) { return (float)__shfl_sync(m, (double)v, src); }
+inline int __shfl_sync(unsigned m, int v, int src) { return (int)__shfl_sync(m, (double)v, src); }
+inline int atomicOr(int* p, int v) { return std::atomic_ref<int>(*p).fetch_or(v); }
+template <class F> void launch(int grid, int block, size_t smem, F f) {
+    gridDim.x = grid; blockDim.x = block;
+    std::vector<unsigned char> dyn(smem + 64);
+    g_dyn_smem = dyn.data();
+    for (int b = 0; b < grid; b++) {
+        std::barrier<> bb(block);
+        g_block_bar = &bb;
+        std::vector<std::barrier<>*> wb;
+        for (int w = 0; w < (block + 31) / 32; w++) wb.push_back(new std::barrier<>(32));
+        g_warp_bar = wb;
+        std::vector<std::thread> ts;
+        for (int t = 0; t < block; t++)
+            ts.emplace_back([&, t, b] { threadIdx.x = t; blockIdx.x = b; f(); });
+        for (auto& th : ts) th.join();
+        for (auto* p : wb) delete p;
+    }
+}
