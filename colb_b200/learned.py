@@ -181,6 +181,7 @@ def run_steps(engine, steps):
 
 TRAIN_SEEDS = tuple(range(1000, 1004))    # chain-net seeds the network is trained on
 EVAL_SEEDS = (500, 501)                    # held out: never seen in training (the benchmark net is seed 0)
+PROBE_SEED, PROBE_STEPS = 123, 40          # the unseen 8 x 8 net of the short check
 
 
 def main():
@@ -210,8 +211,13 @@ def main():
     params, norm, losses = train(X, Y, epochs=args.epochs, seed=args.seed, log=print)
     train_s = time.time() - t1
     ev = evaluate(params, norm, c2_scenes(EVAL_SEEDS), args.eval_steps, log=print)
+    # the short check tests/test_learned.py repeats: an unseen 8 x 8 net, 40 steps
+    probe = evaluate(params, norm, [S.config2_chain_net(n=8, seed=PROBE_SEED)], PROBE_STEPS, rest_from=0)
     meta = dict(pairs=int(len(X)), epochs=args.epochs, final_loss=float(losses[-1]), train_seconds=train_s,
-                train_seeds=seeds, steps=args.steps, seed=args.seed, eval_seeds=list(EVAL_SEEDS), eval=ev)
+                train_seeds=seeds, steps=args.steps, seed=args.seed, eval_seeds=list(EVAL_SEEDS), eval=ev,
+                probe=dict(seed=PROBE_SEED, n=8, steps=PROBE_STEPS, iter_ratio=probe["iter_ratio"],
+                           plain_iters=probe["scenes"][0]["plain"]["iters"],
+                           learned_iters=probe["scenes"][0]["learned"]["iters"]))
     save(args.out, params, norm, meta)
     print(json.dumps({k: v for k, v in meta.items() if k != "eval"}))
     print(f"eval: iterations learned/plain {ev['iter_ratio']:.3f} (resting {ev['iter_ratio_rest']:.3f}), "

@@ -127,28 +127,34 @@ def test_features_match_oracle(which):
 
 @pytest.mark.gpu
 def test_trained_network_gain_over_plain(capsys):
-    """What the shipped network (trained on other chain nets) changes on an
-    unseen one: Newton iterations per step of warm_start 3 against the plain
-    start.  Both must reach the residual every step with no intersection;
-    the ratio is measured and printed, not assumed."""
+    """What the shipped network changes on an unseen 8 x 8 net over 40 steps:
+    Newton iterations per step of warm_start 3 against the plain start.  Both
+    must converge every step with no intersection, and the measured ratio
+    must reproduce the one recorded when the network was trained
+    (colb_b200/learned.py writes it into the model file, meta["probe"]),
+    within 0.1: the test asserts the gain (or loss) that the shipped model
+    claims, whichever it is."""
     from colb_b200 import learned as Lr, params as P, scene as S
     from colb_b200.engine import Engine
-    params, norm, _ = Lr.load()
-    sc = S.config2_chain_net(n=8, seed=123)
+    params, norm, meta = Lr.load()
+    probe = meta.get("probe", dict(n=8, seed=Lr.PROBE_SEED, steps=Lr.PROBE_STEPS, iter_ratio=None))
+    sc = S.config2_chain_net(n=probe["n"], seed=probe["seed"])
     iters = {}
     for ws in (0, 3):
         e = Engine(P.config_params(dt=1.0 / 240.0, warm_start=ws), sc)
         if ws == 3:
             e.set_mlp(params, norm)
         tot = unconv = 0
-        for _ in range(40):
-            rc, st = e.step(1, allow=(-7,))
+        for _ in range(probe["steps"]):
+            rc, st = e.step(1, allow=(-6, -7))
             tot += st.newton_iters
             unconv += st.unconverged
         assert unconv == 0
         assert e.count_intersections() == 0
-        iters[ws] = tot / 40
+        iters[ws] = tot / probe["steps"]
+    ratio = iters[3] / iters[0]
     with capsys.disabled():
         print(f"\nlearned warm start: {iters[3]:.2f} Newton iterations/step vs {iters[0]:.2f} plain "
-              f"(ratio {iters[3] / iters[0]:.2f})")
-    assert iters[3] > 0 and iters[0] > 0
+              f"(ratio {ratio:.2f}; recorded at training {probe['iter_ratio']})")
+    if probe["iter_ratio"] is not None:
+        assert abs(ratio - probe["iter_ratio"]) <= 0.1
