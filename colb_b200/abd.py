@@ -25,6 +25,7 @@ import numpy as np
 
 from . import scene as _scene
 from .engine import Engine
+from ._abi import ABD_ERR_CCD_CAP, ABD_ERR_NEWTON_CAP, ABD_ERR_SOLVER_CAP
 from .params import reference_params
 
 # numpy view of the BDFAffine struct (BDF1.py:11-14, quat_util.py:40-47)
@@ -93,6 +94,7 @@ class NewtonAbd:
         self.frame = 0
         self.profiler = Profiller(max_iters=p.newton_max_iter, frames=frames)
         self.last_stats = None
+        self.last_rc = 0
         self.V = self.compute_V()
 
     # abd_simple.py:64-69
@@ -115,7 +117,11 @@ class NewtonAbd:
 
     # abd.py:674-702
     def step(self):
-        rc, st = self.engine.step(1)
+        # a Krylov, Newton or CCD iteration cap ends the step with the iterate
+        # reached, as the reference's loop does (abd.py:699); the status is
+        # kept in last_rc
+        rc, st = self.engine.step(1, allow=(ABD_ERR_SOLVER_CAP, ABD_ERR_NEWTON_CAP, ABD_ERR_CCD_CAP))
+        self.last_rc = rc
         self.last_stats = st
         res, alpha, ips = self.engine.profile(0)
         n = min(len(res), self.profiler.convergence.shape[1])

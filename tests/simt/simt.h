@@ -50,7 +50,7 @@ inline int __shfl_sync(unsigned m, int v, int src) { return (int)__shfl_sync(m, 
 inline int atomicOr(int* p, int v) { return std::atomic_ref<int>(*p).fetch_or(v); }
 template <class F> void launch(int grid, int block, size_t smem, F f) {
     gridDim.x = grid; blockDim.x = block;
-    std::vector<unsigned char> dyn(smem + 64);
+    std::vector<unsigned char> dyn(smem);
     g_dyn_smem = dyn.data();
     for (int b = 0; b < grid; b++) {
         std::barrier<> bb(block);
