@@ -268,6 +268,18 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_solve(int nsmall, const
 
 
 // ------------------------------------------------------------------ band components
+// 16-byte asynchronous global -> shared copies (cp.async, L1 bypassed): the
+// band kernel fetches the next block row, right-hand side and backward factor
+// column while it computes, so no global load latency sits on its critical
+// path.  Addresses are 16-byte aligned (blocks of 144 doubles, 12-double rows).
+DV void band_cp16(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"((uint32_t)__cvta_generic_to_shared(sdst)), "l"(gsrc)
+                 : "memory");
+}
+DV void band_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+DV void band_cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+DV void band_cp_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 // A component whose bodies, in reverse Cuthill-McKee order, couple only
 // bodies at most BAND_MAX apart is a block band matrix: its Cholesky factor
 // L has the same band.  One CTA factors it with a sliding window of
@@ -302,6 +314,7 @@ constexpr int BAND_THREADS = 256;
 // bases of the window on different banks (144 would start every block on
 // bank 0, and tiles of different blocks read by one warp would conflict)
 constexpr int BAND_BLK = 146;
+constexpr int BAND_CREC = BAND_W * 144 + 12;   // backward record: factor column blocks, then y_k
 
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
 constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
@@ -404,8 +417,8 @@ DV void band_factor_inverse(double* D, double* linv, int* status, double floor, 
 
 __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const int* __restrict__ cptr,
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
-        const double* __restrict__ Ab, const double* __restrict__ g, double* Lg, double* du, int* status,
-        double pivot_floor) {
+        const double* __restrict__ Ab, long long ltot, const double* __restrict__ g, double* Lg, double* du,
+        int* status, double pivot_floor) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* win = (double*)smem_raw;                          // [BAND_W][BAND_W] row-major 12x12 blocks, BAND_BLK apart
     double* stage = win + BAND_W * BAND_W * BAND_BLK;         // [2][BAND_W][144]: next block row / factor column
@@ -415,6 +428,8 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
     double* part = ybuf + 12;                                 // [BAND_MAX][12] (backward)
     double* xs = part + BAND_MAX * 12;                        // [BAND_W][12] latest solution blocks (backward)
     double* dg0 = xs + BAND_W * 12;                           // [BAND_W][12] original diagonal of each window row
+    double* gst = dg0 + BAND_W * 12;                          // [2][12] right-hand side of each staged block row
+    double* cst = gst + 2 * 12;                               // [3][BAND_CREC] backward factor columns and y_k
     __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
     __shared__ int ord[BAND_ORD_MAX];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -426,6 +441,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         const int N = cptr[cc + 1] - cptr[cc], wb = cbw[cc];
         for (int e = tid; e < N; e += blockDim.x) ord[e] = order[cptr[cc] + e];
         double* L = Lg + loff[cc] * 144;                      // Linv_k at (k BAND_W), L(k + d, k) at (k BAND_W + d)
+        double* Y = Lg + ltot * 144 + (loff[cc] / BAND_W) * 12;   // y_k at k * 12
         const double* A = Ab + loff[cc] * 144;                // block A(i, i - d) at (i BAND_W + d)
         __syncthreads();
         auto slot = [&](int i, int j) { return win + ((i % BAND_W) * BAND_W + (j % BAND_W)) * BAND_BLK; };
@@ -438,11 +454,24 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             if (d == 0 && q % 13 == 0) dg0[(i % BAND_W) * 12 + q / 13] = A[(long)e];
         }
         for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = g[12L * ord[e / 12] + e % 12];
-        if (wb + 1 < N) {
-            double* dst = stage + ((wb + 1) & 1) * BAND_W * 144;
-            const double* src = A + (long)(wb + 1) * BAND_W * 144;
-            for (int e = tid; e < (wb + 1) * 144; e += blockDim.x) dst[(wb - e / 144) * 144 + e % 144] = src[e];
-        }
+        // block row m and its right-hand side into staging buffer m & 1; the
+        // stored row holds A(m, m - d) at block d, staged at block wb - d
+        // (column m - wb + (wb - d)); waited for at the end of the next panel
+        auto fetch_row = [&](int m, int t0, int nt) {
+            double* dst = stage + (m & 1) * BAND_W * 144;
+            const double* src = A + (long)m * BAND_W * 144;
+            for (int e = t0; e < (wb + 1) * 72 + 6; e += nt) {
+                if (e < (wb + 1) * 72) {
+                    const int d = e / 72, c = e % 72;
+                    band_cp16(dst + (wb - d) * 144 + 2 * c, src + d * 144 + 2 * c);
+                } else {
+                    const int c = e - (wb + 1) * 72;
+                    band_cp16(gst + (m & 1) * 12 + 2 * c, g + 12L * ord[m] + 2 * c);
+                }
+            }
+            band_cp_commit();
+        };
+        if (wb + 1 < N) fetch_row(wb + 1, tid, blockDim.x);
         __syncthreads();
         if (warp == 0) band_factor_inverse(slot(0, 0), linv, status, pivot_floor, dg0);
         __syncthreads();
@@ -477,8 +506,9 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
 #pragma unroll
                 for (int s = 0; s < 12; s++) if (s <= lane) y += Li[lane * 12 + s] * rk[s];
                 ybuf[lane] = y;
-                du[12L * ord[k] + lane] = y;
+                Y[(long)k * 12 + lane] = y;
             }
+            band_cp_wait_all();              // the block row fetched during the previous column
             __syncthreads();
             // ---- phase 2
             if (warp == 0) {
@@ -551,28 +581,33 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                         slot(m1, k + 1 + q)[x] = src[e];
                         if (q == wb && x % 13 == 0) dg0[(m1 % BAND_W) * 12 + x / 13] = src[e];
                     }
-                    if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = g[12L * ord[m1] + t1];
+                    if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = gst[(m1 & 1) * 12 + t1];
                 }
-                if (m2 < N) {
-                    // block d of the stored row is A(m2, m2 - d): column k + 2 + (wb - d)
-                    double* dst = stage + (m2 & 1) * BAND_W * 144;
-                    const double* src = A + (long)m2 * BAND_W * 144;
-                    for (int e = t1; e < (wb + 1) * 144; e += n1) dst[(wb - e / 144) * 144 + e % 144] = src[e];
-                }
+                if (m2 < N) fetch_row(m2, t1, n1);
             }
             __syncthreads();
         }
-        // backward: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}), y_k in du;
-        // the factor column of k is staged in shared memory while the
-        // previous one is solved
-        {
-            const int k0 = N - 1;
-            for (int e = tid; e < 144; e += blockDim.x) stage[(k0 & 1) * BAND_W * 144 + e] = L[(long)k0 * BAND_W * 144 + e];
-        }
+        // backward: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).  The
+        // record of column k (its factor blocks, then y_k) sits in ring buffer
+        // k % 3 of cst, fetched two columns ahead
+        auto fetch_col = [&](int kk) {
+            const int nkk = min(wb, N - 1 - kk);
+            double* dst = cst + (kk % 3) * BAND_CREC;
+            const double* src = L + (long)kk * BAND_W * 144;
+            for (int e = tid; e < (nkk + 1) * 72 + 6; e += blockDim.x) {
+                if (e < (nkk + 1) * 72) band_cp16(dst + 2 * e, src + 2 * e);
+                else band_cp16(dst + BAND_W * 144 + 2 * (e - (nkk + 1) * 72), Y + (long)kk * 12 + 2 * (e - (nkk + 1) * 72));
+            }
+            band_cp_commit();
+        };
+        fetch_col(N - 1);
+        if (N >= 2) fetch_col(N - 2);
+        band_cp_wait_all();
         __syncthreads();
         for (int k = N - 1; k >= 0; k--) {
             const int nk = min(wb, N - 1 - k);
-            const double* col = stage + (k & 1) * BAND_W * 144;
+            const double* col = cst + (k % 3) * BAND_CREC;
+            if (k >= 2) fetch_col(k - 2);        // into the buffer column k + 1 used
             for (int t = tid; t < 12 * nk; t += blockDim.x) {
                 int d = 1 + t / 12, r = t % 12;              // block L(k + d, k), column r
                 const double* B = col + d * 144;
@@ -582,17 +617,11 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 for (int c = 0; c < 12; c++) acc += B[c * 12 + r] * xi[c];
                 part[(d - 1) * 12 + r] = acc;
             }
-            if (k > 0 && tid >= 128) {                        // stage column k - 1
-                const int nk1 = min(wb, N - k);
-                double* dst = stage + ((k - 1) & 1) * BAND_W * 144;
-                for (int e = tid - 128; e < (nk1 + 1) * 144; e += blockDim.x - 128)
-                    dst[e] = L[(long)(k - 1) * BAND_W * 144 + e];
-            }
             __syncthreads();
             if (warp == 0) {
                 double t = 0.0;
                 if (lane < 12) {
-                    t = du[12L * ord[k] + lane];
+                    t = col[BAND_W * 144 + lane];
                     for (int d = 0; d < nk; d++) t -= part[d * 12 + lane];
                 }
                 // x_k[lane] = sum_{c >= lane} Linv[c][lane] t_c
@@ -604,6 +633,9 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                 }
                 if (lane < 12) { du[12L * ord[k] + lane] = x; xs[(k % BAND_W) * 12 + lane] = x; }
             }
+            // column k - 1 (fetched during column k + 1) must have landed; the
+            // fetch of this column may still be in flight unless it is the last
+            if (k >= 2) band_cp_wait_but_one(); else band_cp_wait_all();
             __syncthreads();
         }
     }
@@ -912,7 +944,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         const int* d_bcptr = d_sbody + small_bodies;
         const int* d_bbw = d_bcptr + nband + 1;
         const int* d_bord = d_bbw + nband;
-        size_t need = (size_t)lblocks * 144 * sizeof(double);
+        size_t need = ((size_t)lblocks * 144 + 12 * band_order.size()) * sizeof(double);
         if (need > D->Lg_bytes) {
             if (D->Lg) cudaFree(D->Lg);
             if (D->Ab) cudaFree(D->Ab);
@@ -927,7 +959,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         // window, staging, inverse diagonal factors, right-hand sides, y_k,
         // backward partial sums and solution blocks
         const size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 +
-                             BAND_MAX * 12 + 2 * BAND_W * 12) * sizeof(double);
+                             BAND_MAX * 12 + 2 * BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * sizeof(double);
         if (!D->band_smem_set) {
             CUDA_TRY(cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             D->band_smem_set = true;
@@ -939,7 +971,8 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         E->launches++;
         int ph = phase_begin(E, PH_BAND);
         k_band_solve<<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, (const double*)D->Ab,
-                                                        E->g, (double*)D->Lg, E->du, D->info, E->mixed ? BAND_PIVOT_FLOOR_MIXED : 0.0);
+                                                        lblocks, E->g, (double*)D->Lg, E->du, D->info,
+                                                        E->mixed ? BAND_PIVOT_FLOOR_MIXED : 0.0);
         // per component: band blocks read, factor written and read back,
         // g read, y and du written and read
         double bytes = 0;

@@ -49,18 +49,20 @@ int main(int argc, char** argv) {
                     Ab[((size_t)i * BAND_W + d) * 144 + r * 12 + c] = M[(12 * i + r) * n + 12 * (i - d) + c];
         std::vector<int> order(N); for (int i = 0; i < N; i++) order[i] = i;
         int cptr[2] = {0, N}, cbw[1] = {wb}; long long loff[1] = {0};
-        std::vector<double> Lg((size_t)N * BAND_W * 144, 0.0), du(n, 0.0);
+        std::vector<double> Lg((size_t)N * BAND_W * 144 + 12 * N, 0.0), du(n, 0.0);
         int status = 0;
         // the kernel's shared-memory layout (as dense.cu sizes it): window,
         // staging, inverse factors, right-hand sides, y_k, partial sums,
         // solution blocks, original diagonals
-        size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_MAX * 12 + 2 * BAND_W * 12) * 8;
-        launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), g.data(), Lg.data(), du.data(), &status, 0.0); });
+        size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_MAX * 12 +
+                       2 * BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * 8;
+        const long long ltot = (long long)N * BAND_W;
+        launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), ltot, g.data(), Lg.data(), du.data(), &status, 0.0); });
         // the mixed-precision pivot floor changes nothing on a well-conditioned SPD matrix
         if (N == 11) {
             std::vector<double> du2(n, 0.0);
             int status2 = 0;
-            launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), g.data(), Lg.data(), du2.data(), &status2, 1e-6); });
+            launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), ltot, g.data(), Lg.data(), du2.data(), &status2, 1e-6); });
             for (int i = 0; i < n; i++) if (du2[i] != du[i]) { printf("pivot floor changed an SPD solve\n"); return 1; }
         }
         // a stiff matrix rounded to FP32 (what a mixed-precision handle
@@ -82,7 +84,7 @@ int main(int argc, char** argv) {
                         Ai[((size_t)i * BAND_W + d) * 144 + r * 12 + c] = (double)(float)Ms[(12 * i + r) * n + 12 * (i - d) + c];
             std::vector<double> du3(n, 0.0);
             int status3 = 0;
-            launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ai.data(), g.data(), Lg.data(), du3.data(), &status3, 1e-6); });
+            launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ai.data(), ltot, g.data(), Lg.data(), du3.data(), &status3, 1e-6); });
             bool fin = true;
             for (double v : du3) fin = fin && std::isfinite(v);
             printf("stiff FP32 N %d: finite %d\n", N, (int)fin);

@@ -3,9 +3,10 @@
 // __syncthreads and __syncwarp are std::barriers, __shfl_sync exchanges
 // through a per-warp array between two warp barriers, and the dynamic shared
 // memory is one host buffer.  Blocks of a grid run one after the other.  It
-// covers what the direct solver's band kernel uses; a kernel that needs
-// anything else (tensor cores, atomics on shared memory, clusters) does not
-// compile against it.
+// covers what the direct solver's band kernel uses (its cp.async helpers are
+// plain copies here, so the emulation checks indexing and barriers, not the
+// timing of asynchronous copies); a kernel that needs anything else (tensor
+// cores, atomics on shared memory, clusters) does not compile against it.
 #pragma once
 #include <barrier>
 #include <thread>
@@ -48,6 +49,11 @@ inline double __shfl_sync(unsigned, double v, int src) {
 inline float __shfl_sync(unsigned m, float v, int src) { return (float)__shfl_sync(m, (double)v, src); }
 inline int __shfl_sync(unsigned m, int v, int src) { return (int)__shfl_sync(m, (double)v, src); }
 inline int atomicOr(int* p, int v) { return std::atomic_ref<int>(*p).fetch_or(v); }
+// cp.async stand-ins: the copy happens at once, so the waits have nothing to wait for
+inline void band_cp16(void* sdst, const void* gsrc) { std::memcpy(sdst, gsrc, 16); }
+inline void band_cp_commit() {}
+inline void band_cp_wait_all() {}
+inline void band_cp_wait_but_one() {}
 template <class F> void launch(int grid, int block, size_t smem, F f) {
     gridDim.x = grid; blockDim.x = block;
     std::vector<unsigned char> dyn(smem);
