@@ -77,7 +77,7 @@ __global__ void k_body_pairs(int nb, const int* __restrict__ bscene, const int* 
         for (int b = a + (self_contact ? 0 : 1) + lane; b < end; b += 32) {
             if (!overlap(al, ah, blo[b], bhi[b])) continue;
             int at = atomicAdd(count, 1);
-            if (at < cap) out[at] = make_int2(a, b);
+            if ((unsigned)at < (unsigned)cap) out[at] = make_int2(a, b);
         }
     }
 }
@@ -128,9 +128,14 @@ DV bool bp_pt_ok(const BpArgs& A, int pv, int t) {
     double L = (double)A.pmag[pv] + (double)fmaxf(A.pmag[a], fmaxf(A.pmag[b], A.pmag[c]));
     return d - L < A.lim;
 }
+// the hit counter stops growing once it passes the capacity (by at most the
+// threads in flight), so a pathological step (a displacement that makes every
+// primitive pair reachable) cannot wrap it; the host then grows the buffer a
+// bounded number of times and reports ABD_ERR_CONTACT_OVERFLOW
 DV void bp_emit(const BpArgs& A, int kind, int a, int b) {
+    if (*(volatile int*)A.count >= A.cap) return;
     int at = atomicAdd(A.count, 1);
-    if (at < A.cap) A.out[at] = ((unsigned long long)kind << 62) | ((unsigned long long)a << 31) | (unsigned long long)b;
+    if ((unsigned)at < (unsigned)A.cap) A.out[at] = ((unsigned long long)kind << 62) | ((unsigned long long)a << 31) | (unsigned long long)b;
 }
 
 // 3. one CTA per body pair

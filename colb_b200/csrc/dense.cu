@@ -298,15 +298,12 @@ DV void band_cp_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memo
 // The 12 dependent pivots of each diagonal block thereby run beside the
 // trailing update instead of before it.  The backward solve walks the
 // columns again: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).
-// The factorization runs in FP64 in both precision modes.  A mixed-precision
-// handle gathers its FP32 blocks into FP64; FP32 roundings of a stiff,
-// PSD-projected Hessian can leave that matrix slightly indefinite, so there a
-// pivot below pivot_floor times the original diagonal entry of its row is
-// raised to that floor (a modified Cholesky: the factor is of the matrix plus
-// a non-negative diagonal, so the increment stays a descent direction; the
-// floor is of the order of the FP32 rounding of the entries).  In FP64 mode
-// pivot_floor is 0 and only a non-positive pivot, which a PSD-projected
-// Hessian does not produce, is replaced by its magnitude.
+// FP64 mode only: FP32 roundings of a stiff PSD-projected Hessian can leave
+// the matrix indefinite (the rounded 12-body blocks of a chain mail in contact
+// have negative eigenvalues), which a Cholesky factorization without pivoting
+// cannot take, so mixed-precision components use the shared-memory and
+// cuSOLVER paths, which fall back to LU.  A non-positive pivot, which a
+// PSD-projected FP64 Hessian does not produce, is replaced by its magnitude.
 constexpr int BAND_MAX = 8;
 constexpr int BAND_W = BAND_MAX + 1;
 constexpr int BAND_THREADS = 256;
@@ -318,7 +315,6 @@ constexpr int BAND_CREC = BAND_W * 144 + 12;   // backward record: factor column
 
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
 constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
-constexpr double BAND_PIVOT_FLOOR_MIXED = 1e-6;   // pivot floor relative to the original diagonal (mixed precision)
 
 // 1/sqrt(d): a single-precision estimate refined by two Newton-Raphson steps
 // r <- r (3 - d r^2) / 2 (each squares the relative error: 2^-23 -> 2^-46 ->
@@ -361,11 +357,9 @@ __global__ void k_band_gather(int npos, const int* __restrict__ pcomp, const int
 // triangle read), written back into D's lower triangle, and
 // its inverse Linv = L^-1 (row-major 12x12, zeros above the diagonal).  Lane
 // r holds row r; each pivot is broadcast, its reciprocal square root computed
-// by every lane, so the 12 columns need no barrier.  A pivot at or below
-// floor * dg[j] (dg: the block's original diagonal, floor 0 in FP64 mode) sets
-// bit 1 of *status and is replaced by that bound, or by its magnitude when
-// the bound is 0.
-DV void band_factor_inverse(double* D, double* linv, int* status, double floor, const double* dg) {
+// by every lane, so the 12 columns need no barrier.  A non-positive pivot
+// sets bit 1 of *status and is replaced by its magnitude.
+DV void band_factor_inverse(double* D, double* linv, int* status) {
     const int lane = threadIdx.x & 31;
     double a[12], rs[12];
 #pragma unroll
@@ -373,11 +367,7 @@ DV void band_factor_inverse(double* D, double* linv, int* status, double floor, 
 #pragma unroll
     for (int j = 0; j < 12; j++) {
         double d = __shfl_sync(0xffffffffu, a[j], j);
-        const double dmin = floor * fabs(dg[j]);
-        if (!(d > dmin)) {
-            if (lane == 0) atomicOr(status, 2);
-            d = dmin > 0.0 ? dmin : fabs(d) + 1e-30;
-        }
+        if (!(d > 0.0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + 1e-30; }
         double r = rsqrt_nr(d);
         rs[j] = r;
         double l = a[j] * r;                      // L[lane][j] for lane > j
@@ -418,7 +408,7 @@ DV void band_factor_inverse(double* D, double* linv, int* status, double floor, 
 __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const int* __restrict__ cptr,
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
         const double* __restrict__ Ab, long long ltot, const double* __restrict__ g, double* Lg, double* du,
-        int* status, double pivot_floor) {
+        int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* win = (double*)smem_raw;                          // [BAND_W][BAND_W] row-major 12x12 blocks, BAND_BLK apart
     double* stage = win + BAND_W * BAND_W * BAND_BLK;         // [2][BAND_W][144]: next block row / factor column
@@ -427,8 +417,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
     double* ybuf = rhs + BAND_W * 12;                         // [12] y_k of the current column
     double* part = ybuf + 12;                                 // [BAND_MAX][12] (backward)
     double* xs = part + BAND_MAX * 12;                        // [BAND_W][12] latest solution blocks (backward)
-    double* dg0 = xs + BAND_W * 12;                           // [BAND_W][12] original diagonal of each window row
-    double* gst = dg0 + BAND_W * 12;                          // [2][12] right-hand side of each staged block row
+    double* gst = xs + BAND_W * 12;                           // [2][12] right-hand side of each staged block row
     double* cst = gst + 2 * 12;                               // [3][BAND_CREC] backward factor columns and y_k
     __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
     __shared__ int ord[BAND_ORD_MAX];
@@ -451,7 +440,6 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         for (int e = tid; e < (r0 + 1) * BAND_W * 144; e += blockDim.x) {
             int i = e / (BAND_W * 144), d = (e / 144) % BAND_W, q = e % 144;
             if (d <= i) slot(i, i - d)[q] = A[(long)e];
-            if (d == 0 && q % 13 == 0) dg0[(i % BAND_W) * 12 + q / 13] = A[(long)e];
         }
         for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = g[12L * ord[e / 12] + e % 12];
         // block row m and its right-hand side into staging buffer m & 1; the
@@ -473,7 +461,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
         };
         if (wb + 1 < N) fetch_row(wb + 1, tid, blockDim.x);
         __syncthreads();
-        if (warp == 0) band_factor_inverse(slot(0, 0), linv, status, pivot_floor, dg0);
+        if (warp == 0) band_factor_inverse(slot(0, 0), linv, status);
         __syncthreads();
         for (int k = 0; k < N; k++) {
             const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
@@ -525,7 +513,7 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                         D[r * 12 + c] -= acc;
                     }
                     __syncwarp();
-                    band_factor_inverse(D, linv + ((k + 1) & 1) * 144, status, pivot_floor, dg0 + ((k + 1) % BAND_W) * 12);
+                    band_factor_inverse(D, linv + ((k + 1) & 1) * 144, status);
                 }
             } else {
                 const int t1 = tid - 32, n1 = blockDim.x - 32;
@@ -579,7 +567,6 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     for (int e = t1; e < (wb + 1) * 144; e += n1) {
                         int q = e / 144, x = e % 144;             // block q: column k + 1 + q
                         slot(m1, k + 1 + q)[x] = src[e];
-                        if (q == wb && x % 13 == 0) dg0[(m1 % BAND_W) * 12 + x / 13] = src[e];
                     }
                     if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = gst[(m1 & 1) * 12 + t1];
                 }
@@ -867,10 +854,12 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     for (int b = 0; b < nb; b++) {
         int r = find(b), sz = D->size[r];
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
-        // a single CTA walks the band sequentially, so cuSOLVER (all SMs) is
-        // faster for a component above BAND_PREFER_MAX bodies while few such
-        // components exist
-        if (D->root[r] == -1 && projected &&
+        // FP32 roundings of a stiff projected Hessian can make it indefinite
+        // (the band Cholesky has no pivoting), so the band path runs in FP64
+        // mode only; a single CTA walks the band sequentially, so cuSOLVER
+        // (all SMs) is faster for a component above BAND_PREFER_MAX bodies
+        // while few such components exist
+        if (D->root[r] == -1 && projected && !E->mixed &&
             (sz <= BAND_PREFER_MAX || (int)large_n.size() >= MAX_LARGE_COMPONENTS / 2)) {
             int bw = rcm(r, ord);
             if (bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
@@ -959,7 +948,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         // window, staging, inverse diagonal factors, right-hand sides, y_k,
         // backward partial sums and solution blocks
         const size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 +
-                             BAND_MAX * 12 + 2 * BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * sizeof(double);
+                             BAND_MAX * 12 + BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * sizeof(double);
         if (!D->band_smem_set) {
             CUDA_TRY(cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             D->band_smem_set = true;
@@ -971,8 +960,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         E->launches++;
         int ph = phase_begin(E, PH_BAND);
         k_band_solve<<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, (const double*)D->Ab,
-                                                        lblocks, E->g, (double*)D->Lg, E->du, D->info,
-                                                        E->mixed ? BAND_PIVOT_FLOOR_MIXED : 0.0);
+                                                        lblocks, E->g, (double*)D->Lg, E->du, D->info);
         // per component: band blocks read, factor written and read back,
         // g read, y and du written and read
         double bytes = 0;

@@ -224,7 +224,7 @@ __global__ void k_ee_pairs(int ne, GridView GV, Geo G, const float4* __restrict_
             if (!ee_test(G, ii, j, f32, self_contact, filt, s, t, d)) return;
             if (mode == 1) {
                 int at = base + c;
-                if (at < cap) out[at] = make_int4(ABD_CONTACT_EE, ii, j, 0);
+                if ((unsigned)at < (unsigned)cap) out[at] = make_int4(ABD_CONTACT_EE, ii, j, 0);
                 else *overflow = 1;
             }
             c++;
@@ -253,7 +253,7 @@ __global__ void k_pt_pairs(int nv, GridView GV, Geo G, const float4* __restrict_
             if (!pt_test(G, pp, t, self_contact, filt)) return;
             if (mode == 1) {
                 int at = base + c;
-                if (at < cap) out[at] = make_int4(ABD_CONTACT_PT, pp, t, 0);
+                if ((unsigned)at < (unsigned)cap) out[at] = make_int4(ABD_CONTACT_PT, pp, t, 0);
                 else *overflow = 1;
             }
             c++;
@@ -284,7 +284,7 @@ __global__ void k_pg_pairs(int nv, Geo G, const int* __restrict__ vscene, double
             if (!(d < filt)) continue;
             if (mode == 1) {
                 int at = base + c;
-                if (at < cap) out[at] = make_int4(ABD_CONTACT_PG, (int)v, pl, 0);
+                if ((unsigned)at < (unsigned)cap) out[at] = make_int4(ABD_CONTACT_PG, (int)v, pl, 0);
                 else *overflow = 1;
             }
             c++;

@@ -400,6 +400,10 @@ static int resolved_solver(const Engine* E) {
     return kind;
 }
 
+// an increment entry above this (scene units for positions, dimensionless for
+// the affine rows) is no Newton step of a physical scene: it is taken as an
+// FP32 breakdown like a non-finite one
+constexpr double DU_GUARD_MAX = 1e6;
 // Mixed precision: a scene whose FP32 solve left a non-finite entry in du
 // takes the block-Jacobi direction du_b = D_b^-1 g_b instead (every body's
 // inverse diagonal block is finite: a singular block inverts to the
@@ -408,7 +412,7 @@ __global__ void k_du_nonfinite(int nb, const double* __restrict__ du, const int*
                                const int* __restrict__ done, int* bad) {
     GS_LOOP(i, 12L * nb) {
         int s = bscene[i / 12];
-        if (!done[s] && !isfinite(du[i])) bad[s] = 1;
+        if (!done[s] && !(fabs(du[i]) <= DU_GUARD_MAX)) bad[s] = 1;     // non-finite or absurd
     }
 }
 __global__ void k_du_jacobi(int nb, const float* __restrict__ dinv, const double* __restrict__ g,

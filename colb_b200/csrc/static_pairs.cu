@@ -132,7 +132,7 @@ __global__ void k_st_pairs(int ne, GridView GV, const double* __restrict__ x, co
             if (mode == 1) {
                 // the partner edge index goes in slot 2 until the segment is sorted
                 int at = base + c;
-                if (at < cap) { out4[4*at] = a0; out4[4*at+1] = a1; out4[4*at+2] = j; out4[4*at+3] = -1; }
+                if ((unsigned)at < (unsigned)cap) { out4[4*at] = a0; out4[4*at+1] = a1; out4[4*at+2] = j; out4[4*at+3] = -1; }
             }
             c++;
         });

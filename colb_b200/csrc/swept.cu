@@ -132,7 +132,7 @@ __global__ void k_sw_ee(int ne, GridView GV, Geo G, const float* __restrict__ pm
                 if (a.x == b.x || a.x == b.y || a.y == b.x || a.y == b.y) return;
                 if (!self_contact && G.vbody[a.x] == G.vbody[b.x]) return;
                 if (!ee_may_reach(G, pmag, ii, j, lim)) return;
-                if (mode == 1) { int at = base + c; if (at < cap) out[at] = make_int4(ABD_CONTACT_EE, ii, j, 0); else *overflow = 1; }
+                if (mode == 1) { int at = base + c; if ((unsigned)at < (unsigned)cap) out[at] = make_int4(ABD_CONTACT_EE, ii, j, 0); else *overflow = 1; }
                 c++;
             });
         }
@@ -157,7 +157,7 @@ __global__ void k_sw_pt(int nv, GridView GV, Geo G, const float* __restrict__ pm
                 if (pp == a || pp == G.tris[3*t+1] || pp == G.tris[3*t+2]) return;
                 if (!self_contact && G.vbody[pp] == G.vbody[a]) return;
                 if (!pt_may_reach(G, pmag, pp, t, lim)) return;
-                if (mode == 1) { int at = base + c; if (at < cap) out[at] = make_int4(ABD_CONTACT_PT, pp, t, 0); else *overflow = 1; }
+                if (mode == 1) { int at = base + c; if ((unsigned)at < (unsigned)cap) out[at] = make_int4(ABD_CONTACT_PT, pp, t, 0); else *overflow = 1; }
                 c++;
             });
         }
@@ -172,7 +172,8 @@ __global__ void k_sw_count(const int* off_ee, int ne, const int* off_pt, int npt
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         int a = off_ee ? off_ee[ne] : 0, b = off_pt ? off_pt[npt] : 0;
         cnt->n_sw_ee = a; cnt->n_sw = a + b;
-        if (a + b > cap) cnt->sw_overflow = 1;
+        // a scan whose sum passed the int range shows as a negative total
+        if (a < 0 || b < 0 || (long long)a + b > cap) cnt->sw_overflow = 1;
     }
 }
 
@@ -385,7 +386,7 @@ __global__ void k_list_scatter(int n, const int4* __restrict__ list, const int* 
                                int4* out, const int* __restrict__ n_ee_dev, Counters* cnt, int cap) {
     const int n_ee_list = *n_ee_dev;
     GS_LOOP(c, n) {
-        if (flag[c]) { int at = off[c]; if (at < cap) out[at] = list[c]; }
+        if (flag[c]) { int at = off[c]; if ((unsigned)at < (unsigned)cap) out[at] = list[c]; }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         cnt->n_ee = off[n_ee_list];

@@ -53,43 +53,11 @@ int main(int argc, char** argv) {
         int status = 0;
         // the kernel's shared-memory layout (as dense.cu sizes it): window,
         // staging, inverse factors, right-hand sides, y_k, partial sums,
-        // solution blocks, original diagonals
+        // solution blocks, staged right-hand sides, backward records
         size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_MAX * 12 +
-                       2 * BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * 8;
+                       BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * 8;
         const long long ltot = (long long)N * BAND_W;
-        launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), ltot, g.data(), Lg.data(), du.data(), &status, 0.0); });
-        // the mixed-precision pivot floor changes nothing on a well-conditioned SPD matrix
-        if (N == 11) {
-            std::vector<double> du2(n, 0.0);
-            int status2 = 0;
-            launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), ltot, g.data(), Lg.data(), du2.data(), &status2, 1e-6); });
-            for (int i = 0; i < n; i++) if (du2[i] != du[i]) { printf("pivot floor changed an SPD solve\n"); return 1; }
-        }
-        // a stiff matrix rounded to FP32 (what a mixed-precision handle
-        // gathers): stiff couplings 1e9 (v v^T, v = e_a - e_b between
-        // neighbouring bodies) over O(1) entries; after rounding, the Schur
-        // complements along the stiff directions lose their O(1) part and a
-        // pivot can come out negative.  With the floor every pivot stays
-        // positive and the solution finite.
-        if (N == 5) {
-            std::vector<double> Ms = M;
-            for (int i = 0; i + 1 < N; i++) {
-                int a = 12 * i + 3, b = 12 * (i + 1) + 3;
-                Ms[a * n + a] += 1e9; Ms[b * n + b] += 1e9; Ms[a * n + b] -= 1e9; Ms[b * n + a] -= 1e9;
-            }
-            std::vector<double> Ai(Ab.size(), 0.0);
-            for (int i = 0; i < N; i++)
-                for (int d = 0; d <= std::min(wb, i); d++)
-                    for (int r = 0; r < 12; r++) for (int c = 0; c < 12; c++)
-                        Ai[((size_t)i * BAND_W + d) * 144 + r * 12 + c] = (double)(float)Ms[(12 * i + r) * n + 12 * (i - d) + c];
-            std::vector<double> du3(n, 0.0);
-            int status3 = 0;
-            launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ai.data(), ltot, g.data(), Lg.data(), du3.data(), &status3, 1e-6); });
-            bool fin = true;
-            for (double v : du3) fin = fin && std::isfinite(v);
-            printf("stiff FP32 N %d: finite %d\n", N, (int)fin);
-            if (!fin) return 1;
-        }
+        launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), ltot, g.data(), Lg.data(), du.data(), &status); });
         auto ref = dense_solve(M, g, n);
         double err = 0, sc = 0;
         for (int i = 0; i < n; i++) { err = std::max(err, std::fabs(du[i] - ref[i])); sc = std::max(sc, std::fabs(ref[i])); }

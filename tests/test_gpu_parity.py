@@ -123,16 +123,6 @@ def test_direct_solve_by_components(chain_scene, chain_pairs, hess_mode, precisi
         g, H = o.assemble()
         ref = np.linalg.solve(H, g)
         assert it == 1
-        if precision == 1 and hess_mode == 1 and st is None:
-            # chain mail in contact, mixed precision: the FP32 blocks of
-            # these stiff systems are indefinite (their smallest eigenvalue
-            # is negative once rounded), so the band path's modified
-            # Cholesky factors the matrix plus a diagonal and returns a
-            # descent direction, not a backward-stable solve of the rounded
-            # matrix; the mixed trajectories are checked against FP64
-            # elsewhere (within 1e-4)
-            assert np.all(np.isfinite(du)) and g @ du > 0
-            continue
         # backward error of a stable factorization, and the forward error it implies
         n = len(g)
         back = np.abs(H @ du - g).max() / (np.abs(H).max() * np.abs(du).max() + np.abs(g).max())
