@@ -279,25 +279,34 @@ DV void band_cp16(void* sdst, const void* gsrc) {
 DV void band_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 DV void band_cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 DV void band_cp_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// named CTA barrier `id` over `n` threads (counted per thread, so a warp
+// may reach it diverged): arrive only, which publishes this thread's earlier
+// shared-memory writes to the waiting threads, or arrive and wait
+DV void band_bar_arrive(int id, int n) { asm volatile("barrier.arrive %0, %1;" :: "r"(id), "r"(n) : "memory"); }
+DV void band_bar_sync(int id, int n) { asm volatile("barrier.sync %0, %1;" :: "r"(id), "r"(n) : "memory"); }
 
 // A component whose bodies, in reverse Cuthill-McKee order, couple only
 // bodies at most BAND_MAX apart is a block band matrix: its Cholesky factor
 // L has the same band.  One CTA factors it with a sliding window of
 // (BAND_MAX + 1)^2 12x12 blocks in shared memory, all band components in
-// one launch, with no host synchronisation.  Block column k takes two
-// phases, each closed by a block barrier:
-//   1. panel: L_ik = A_ik Linv_k^T for the blocks below the diagonal, where
-//      Linv_k = L_kk^-1 is kept explicitly, so every entry is an
-//      independent dot product; forward elimination y_k = Linv_k g_k;
-//   2. warp 0 applies column k to the next diagonal block
-//      (A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T), factors it in registers and
-//      inverts the factor (Linv_{k+1}), while warps 1..7 apply column k to
-//      the rest of the window (A_ij -= L_ik L_jk^T), eliminate the
-//      right-hand sides below, write the factor column to global scratch
-//      and bring the next block row into the window.
-// The 12 dependent pivots of each diagonal block thereby run beside the
-// trailing update instead of before it.  The backward solve walks the
-// columns again: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).
+// one launch, with no host synchronisation.  The inverse diagonal factors
+// Linv_k = L_kk^-1 are kept explicitly, so every panel entry is an
+// independent dot product.  Block column k:
+//   1. panel L_ik = A_ik Linv_k^T: warp 0 computes block row k + 1 and
+//      signals it at a named barrier without waiting; warps 1..6 compute
+//      the rows below, warp 7 the forward elimination y_k = Linv_k g_k;
+//   2. warp 0 goes straight on: A_{k+1,k+1} - L_{k+1,k} L_{k+1,k}^T into
+//      registers, then its Cholesky factor and inverse (Linv_{k+1}) in one
+//      sweep of 12 pivots; warps 1..7, once the whole panel is there (named
+//      barrier), apply column k to the rest of the window
+//      (A_ij -= L_ik L_jk^T), eliminate the right-hand sides below, write
+//      the factor column to global scratch and bring the next block row
+//      into the window.
+// One block barrier closes the column.  Warp 0's chain (one panel block
+// row, the diagonal update, 12 pivots) is the critical path.  The backward
+// solve, x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}), is one short
+// dependent chain per column and runs on warp 0 alone under warp-level
+// synchronisation, each factor column prefetched two columns ahead.
 // FP64 mode only: FP32 roundings of a stiff PSD-projected Hessian can leave
 // the matrix indefinite (the rounded 12-body blocks of a chain mail in contact
 // have negative eigenvalues), which a Cholesky factorization without pivoting
@@ -312,21 +321,28 @@ constexpr int BAND_THREADS = 256;
 // bank 0, and tiles of different blocks read by one warp would conflict)
 constexpr int BAND_BLK = 146;
 constexpr int BAND_CREC = BAND_W * 144 + 12;   // backward record: factor column blocks, then y_k
+// dynamic shared memory of k_band_solve in doubles: window, staged block
+// rows, inverse diagonal factors, right-hand sides, y_k, solution blocks,
+// staged right-hand sides, backward records
+constexpr int band_smem_doubles() {
+    return BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_W * 12 + 2 * 12 +
+           3 * BAND_CREC;
+}
 
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
 constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
 
-// 1/sqrt(d): a single-precision estimate refined by two Newton-Raphson steps
-// r <- r (3 - d r^2) / 2 (each squares the relative error: 2^-23 -> 2^-46 ->
-// below double rounding); outside the single-precision range the
+// 1/sqrt(d): the single-precision estimate r0 (relative error below 2^-22)
+// refined by one third-order Householder step.  With e = 1 - d r0^2,
+// 1/sqrt(d) = r0 (1 - e)^(-1/2) = r0 (1 + e/2 + 3 e^2/8 + O(e^3)): the
+// truncation is below 2^-66, so the result is good to a few ulps after four
+// dependent FP64 operations.  Outside the single-precision range the
 // double-precision rsqrt is used.
 DV double rsqrt_nr(double d) {
     if (!(d > 1e-30 && d < 1e30)) return rsqrt(d);
-    double r = (double)rsqrtf((float)d);
-    double h = 0.5 * d;
-    r = r * (1.5 - h * r * r);
-    r = r * (1.5 - h * r * r);
-    return r;
+    const double r0 = (double)rsqrtf((float)d);
+    const double e = fma(-d * r0, r0, 1.0);
+    return fma(r0 * e, fma(0.375, e, 0.5), r0);
 }
 
 // Band blocks of every band component, contiguous and in FP64: A(i, i - d)
@@ -353,75 +369,95 @@ __global__ void k_band_gather(int npos, const int* __restrict__ pcomp, const int
     }
 }
 
-// Warp-wide: Cholesky factor of the 12x12 SPD block D (row-major, lower
-// triangle read), written back into D's lower triangle, and
-// its inverse Linv = L^-1 (row-major 12x12, zeros above the diagonal).  Lane
-// r holds row r; each pivot is broadcast, its reciprocal square root computed
-// by every lane, so the 12 columns need no barrier.  A non-positive pivot
-// sets bit 1 of *status and is replaced by its magnitude.
-DV void band_factor_inverse(double* D, double* linv, int* status) {
+// Warp-wide Cholesky factorization and inversion of a 12x12 SPD block in
+// one sweep of its 12 pivots.  On entry lane i < 12 holds row i of the
+// (symmetric) block in a[]; on exit it holds row i of W = L^-1, zeros right
+// of the diagonal, where L L^T is the block.  Step j: lane j owns the pivot
+// d_j = a[j]; every lane i > j forms t = a_ij / d_j and subtracts t times
+// lane j's row.  Right of column j that row is the remaining block row, so
+// this is the Schur update a_ic -= a_ij a_jc / d_j; left of column j it is
+// row j of the unscaled inverse w, so this is the forward substitution
+// w_i -= (L_ij / L_jj) w_j of L w = I; slot j itself becomes w_ij = -t.
+// Finally W_i = w_i / sqrt(d_i).  Lane j's row is final one step before it
+// is needed, so each pivot costs one reciprocal square root and one
+// broadcast on the dependent chain.  A non-positive pivot sets bit 1 of
+// *status and is replaced by its magnitude.
+DV void band_chol_inverse_rows(double (&a)[12], int* status) {
     const int lane = threadIdx.x & 31;
-    double a[12], rs[12];
-#pragma unroll
-    for (int c = 0; c < 12; c++) a[c] = lane < 12 ? D[lane * 12 + c] : 0.0;
+    double rown = 0.0;
 #pragma unroll
     for (int j = 0; j < 12; j++) {
-        double d = __shfl_sync(0xffffffffu, a[j], j);
-        if (!(d > 0.0)) { if (lane == 0) atomicOr(status, 2); d = fabs(d) + 1e-30; }
-        double r = rsqrt_nr(d);
-        rs[j] = r;
-        double l = a[j] * r;                      // L[lane][j] for lane > j
-        if (lane == j) a[j] = d * r;
-        if (lane > j) a[j] = l;
-        // every index static, so a[] stays in registers
+        double s = 0.0;
+        if (lane == j) {
+            double d = a[j];
+            if (!(d > 0.0)) { atomicOr(status, 2); d = fabs(d) + 1e-30; }
+            rown = rsqrt_nr(d);
+            s = rown * rown;
+        }
+        if (j < 11) {
+            s = __shfl_sync(0xffffffffu, s, j);
+            const bool upd = lane > j && lane < 12;
+            const double t = a[j] * s;
 #pragma unroll
-        for (int c = 0; c < 12; c++) {
-            double lc = __shfl_sync(0xffffffffu, l, c);   // L[c][j] for c > j
-            if (c > j && lane > j) a[c] -= l * lc;
+            for (int c = 0; c < 12; c++) {
+                if (c == j) continue;
+                const double v = __shfl_sync(0xffffffffu, a[c], j);
+                if (upd) a[c] = fma(-t, v, a[c]);
+            }
+            if (upd) a[j] = -t;
+        }
+        if (lane == j) {
+            a[j] = 1.0;
+#pragma unroll
+            for (int c = j + 1; c < 12; c++) a[c] = 0.0;
         }
     }
-    if (lane < 12) {
 #pragma unroll
-        for (int c = 0; c < 12; c++) if (c <= lane) D[lane * 12 + c] = a[c];
+    for (int c = 0; c < 12; c++) a[c] *= rown;
+}
+
+// Panel rows in place: R (one row of a block below the diagonal) becomes
+// R Linv^T, i.e. entry c = sum_{s <= c} R[s] Linv[c][s].  Two lanes (adjacent
+// or 12 apart) share a row and write six entries each; every lane of the
+// warp must call it, `act` says whether this lane has a row.
+DV void band_panel_row(double* R, const double* Li, int half, bool act) {
+    double v[12];
+    if (act) {
+#pragma unroll
+        for (int s = 0; s < 12; s++) v[s] = R[s];
     }
     __syncwarp();
-    // column `lane` of L^-1 by forward substitution, L[r][s] broadcast from
-    // shared memory: x[r] = (delta(r, lane) - sum_{s<r} L[r][s] x[s]) / L[r][r]
-    double x[12];
+    if (act) {
 #pragma unroll
-    for (int r = 0; r < 12; r++) {
-        double acc0 = (lane == r) ? 1.0 : 0.0, acc1 = 0.0;
+        for (int c6 = 0; c6 < 6; c6++) {
+            const int c = half * 6 + c6;
+            double acc = 0.0;
 #pragma unroll
-        for (int s = 0; s < r; s++) {
-            double Lrs = D[r * 12 + s];
-            if (s & 1) acc1 -= Lrs * x[s]; else acc0 -= Lrs * x[s];
+            for (int s = 0; s < 12; s++) if (s <= c) acc += v[s] * Li[c * 12 + s];
+            R[c] = acc;
         }
-        x[r] = (acc0 + acc1) * rs[r];
-    }
-    if (lane < 12) {
-#pragma unroll
-        for (int r = 0; r < 12; r++) linv[r * 12 + lane] = x[r];
     }
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const int* __restrict__ cptr,
+// one CTA per SM (its shared memory allows no second), so the register cap is set for one
+__global__ void __launch_bounds__(BAND_THREADS, 1) k_band_solve(int ncomp, const int* __restrict__ cptr,
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
         const double* __restrict__ Ab, long long ltot, const double* __restrict__ g, double* Lg, double* du,
         int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* win = (double*)smem_raw;                          // [BAND_W][BAND_W] row-major 12x12 blocks, BAND_BLK apart
-    double* stage = win + BAND_W * BAND_W * BAND_BLK;         // [2][BAND_W][144]: next block row / factor column
+    double* stage = win + BAND_W * BAND_W * BAND_BLK;         // [2][BAND_W][144]: next block row
     double* linv = stage + 2 * BAND_W * 144;                  // [2][144] inverse diagonal factors
     double* rhs = linv + 2 * 144;                             // [BAND_W][12]
     double* ybuf = rhs + BAND_W * 12;                         // [12] y_k of the current column
-    double* part = ybuf + 12;                                 // [BAND_MAX][12] (backward)
-    double* xs = part + BAND_MAX * 12;                        // [BAND_W][12] latest solution blocks (backward)
+    double* xs = ybuf + 12;                                   // [BAND_W][12] latest solution blocks (backward)
     double* gst = xs + BAND_W * 12;                           // [2][12] right-hand side of each staged block row
     double* cst = gst + 2 * 12;                               // [3][BAND_CREC] backward factor columns and y_k
     __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
     __shared__ int ord[BAND_ORD_MAX];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int t1 = tid - 32, n1 = blockDim.x - 32;            // thread index among warps 1..7
     if (tid < BAND_MAX * (BAND_MAX + 1) / 2) {
         int a = 0; while ((a + 1) * (a + 2) / 2 <= tid) a++;
         tri_a[tid] = (unsigned char)a; tri_b[tid] = (unsigned char)(tid - a * (a + 1) / 2);
@@ -442,13 +478,14 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             if (d <= i) slot(i, i - d)[q] = A[(long)e];
         }
         for (int e = tid; e < (r0 + 1) * 12; e += blockDim.x) rhs[(e / 12) * 12 + e % 12] = g[12L * ord[e / 12] + e % 12];
-        // block row m and its right-hand side into staging buffer m & 1; the
-        // stored row holds A(m, m - d) at block d, staged at block wb - d
-        // (column m - wb + (wb - d)); waited for at the end of the next panel
-        auto fetch_row = [&](int m, int t0, int nt) {
+        // block row m and its right-hand side into staging buffer m & 1 by
+        // warps 1..7; the stored row holds A(m, m - d) at block d, staged at
+        // block wb - d (column m - wb + (wb - d)); the same threads wait for
+        // it before the named barrier of the next column
+        auto fetch_row = [&](int m) {
             double* dst = stage + (m & 1) * BAND_W * 144;
             const double* src = A + (long)m * BAND_W * 144;
-            for (int e = t0; e < (wb + 1) * 72 + 6; e += nt) {
+            for (int e = t1; e < (wb + 1) * 72 + 6; e += n1) {
                 if (e < (wb + 1) * 72) {
                     const int d = e / 72, c = e % 72;
                     band_cp16(dst + (wb - d) * 144 + 2 * c, src + d * 144 + 2 * c);
@@ -459,64 +496,82 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
             }
             band_cp_commit();
         };
-        if (wb + 1 < N) fetch_row(wb + 1, tid, blockDim.x);
+        if (warp > 0 && wb + 1 < N) fetch_row(wb + 1);
         __syncthreads();
-        if (warp == 0) band_factor_inverse(slot(0, 0), linv, status);
+        if (warp == 0) {
+            const double* D = slot(0, 0);
+            double a[12];
+#pragma unroll
+            for (int c = 0; c < 12; c++) a[c] = lane < 12 ? D[lane * 12 + c] : 0.0;
+            band_chol_inverse_rows(a, status);
+            if (lane < 12) {
+#pragma unroll
+                for (int c = 0; c < 12; c++) linv[lane * 12 + c] = a[c];
+            }
+        }
         __syncthreads();
+        // with a body bandwidth wb >= 1 (a connected component of two or more
+        // bodies), every column but the last has nk >= 1 blocks below the diagonal
         for (int k = 0; k < N; k++) {
             const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
             const double* Li = linv + (k & 1) * 144;
-            // ---- phase 1: panel L_ik = A_ik Linv_k^T (two lanes per block
-            // row: each loads the whole row, then writes six entries), and y_k
-            if (warp < 6) {
-                const int q = tid >> 1, half = tid & 1;
-                const bool act = q < 12 * nk;
-                double v[12];
-                double* R = act ? slot(k + 1 + q / 12, k) + (q % 12) * 12 : nullptr;
-                if (act) {
+            if (warp == 0) {
+                // panel block row k + 1 (lanes r and r + 12 share row r), signalled to warps 1..7
+                const int r = lane % 12, half = lane / 12;
+                double* P = slot(k + 1, k);
+                if (nk > 0) band_panel_row(P + r * 12, Li, half, lane < 24);
+                band_bar_arrive(1, blockDim.x);
+                if (nk > 0) {
+                    // row r of A_{k+1,k+1} - L_{k+1,k} L_{k+1,k}^T: lane r forms entries 0..5,
+                    // lane r + 12 entries 6..11 and passes them to lane r
+                    const double* Dk = slot(k + 1, k + 1);
+                    double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                    if (lane < 24) {
+                        double lr[12];
 #pragma unroll
-                    for (int s = 0; s < 12; s++) v[s] = R[s];
-                }
-                __syncwarp();
-                if (act) {
+                        for (int s = 0; s < 12; s++) lr[s] = P[r * 12 + s];
+#pragma unroll
+                        for (int c6 = 0; c6 < 6; c6++) {
+                            const int c = half * 6 + c6;
+                            double acc0 = Dk[r * 12 + c], acc1 = 0.0;
+#pragma unroll
+                            for (int s = 0; s < 12; s += 2) {
+                                acc0 = fma(-lr[s], P[c * 12 + s], acc0);
+                                acc1 = fma(-lr[s + 1], P[c * 12 + s + 1], acc1);
+                            }
+                            h[c6] = acc0 + acc1;
+                        }
+                    }
+                    double a[12];
 #pragma unroll
                     for (int c6 = 0; c6 < 6; c6++) {
-                        const int c = half * 6 + c6;
-                        double acc = 0.0;
-#pragma unroll
-                        for (int s = 0; s < 12; s++) if (s <= c) acc += v[s] * Li[c * 12 + s];
-                        R[c] = acc;
+                        const double o = __shfl_sync(0xffffffffu, h[c6], (lane + 12) & 31);
+                        a[c6] = lane < 12 ? h[c6] : 0.0;
+                        a[6 + c6] = lane < 12 ? o : 0.0;
                     }
-                }
-            } else if (warp == 6 && lane < 12) {
-                const double* rk = rhs + (k % BAND_W) * 12;
-                double y = 0.0;
+                    band_chol_inverse_rows(a, status);
+                    if (lane < 12) {
+                        double* Ln = linv + ((k + 1) & 1) * 144;
 #pragma unroll
-                for (int s = 0; s < 12; s++) if (s <= lane) y += Li[lane * 12 + s] * rk[s];
-                ybuf[lane] = y;
-                Y[(long)k * 12 + lane] = y;
-            }
-            band_cp_wait_all();              // the block row fetched during the previous column
-            __syncthreads();
-            // ---- phase 2
-            if (warp == 0) {
-                if (k + 1 < N) {
-                    // A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T (lower triangle), then factor and invert
-                    double* D = slot(k + 1, k + 1);
-                    const double* Lr = slot(k + 1, k);
-                    for (int e = lane; e < 78; e += 32) {
-                        int r = 0; while ((r + 1) * (r + 2) / 2 <= e) r++;
-                        const int c = e - r * (r + 1) / 2;
-                        double acc = 0.0;
-#pragma unroll
-                        for (int s = 0; s < 12; s++) acc += Lr[r * 12 + s] * Lr[c * 12 + s];
-                        D[r * 12 + c] -= acc;
+                        for (int c = 0; c < 12; c++) Ln[lane * 12 + c] = a[c];
                     }
-                    __syncwarp();
-                    band_factor_inverse(D, linv + ((k + 1) & 1) * 144, status);
                 }
             } else {
-                const int t1 = tid - 32, n1 = blockDim.x - 32;
+                if (warp < 7) {
+                    // panel rows of blocks k + 2 .. k + nk, two adjacent lanes per row
+                    const int q = 12 + (t1 >> 1);
+                    const bool act = q < 12 * nk;
+                    band_panel_row(act ? slot(k + 1 + q / 12, k) + (q % 12) * 12 : win, Li, t1 & 1, act);
+                } else if (lane < 12) {
+                    const double* rk = rhs + (k % BAND_W) * 12;
+                    double y = 0.0;
+#pragma unroll
+                    for (int s = 0; s < 12; s++) if (s <= lane) y += Li[lane * 12 + s] * rk[s];
+                    ybuf[lane] = y;
+                    Y[(long)k * 12 + lane] = y;
+                }
+                band_cp_wait_all();              // this thread's copies of the staged block row
+                band_bar_sync(1, blockDim.x);    // panel (warp 0's row included), y_k and the staged row are there
                 // A_ij -= L_ik L_jk^T over the window in 3 x 4 tiles (12 per
                 // block pair); pair 0, (k+1, k+1), is warp 0's
                 const int npair = nk * (nk + 1) / 2;
@@ -560,7 +615,8 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     L[((long)k * BAND_W + d) * 144 + q] = d == 0 ? Li[q] : slot(k + d, k)[q];
                 }
                 // block row k + 1 + wb enters the window (staged during the
-                // previous column), and row k + 2 + wb is fetched
+                // previous column; its ring row is that of row k, free now),
+                // and row k + 2 + wb is fetched
                 const int m1 = k + 1 + wb, m2 = k + 2 + wb;
                 if (m1 < N) {
                     const double* src = stage + (m1 & 1) * BAND_W * 144;
@@ -570,61 +626,63 @@ __global__ void __launch_bounds__(BAND_THREADS) k_band_solve(int ncomp, const in
                     }
                     if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = gst[(m1 & 1) * 12 + t1];
                 }
-                if (m2 < N) fetch_row(m2, t1, n1);
+                if (m2 < N) fetch_row(m2);
             }
             __syncthreads();
         }
-        // backward: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).  The
-        // record of column k (its factor blocks, then y_k) sits in ring buffer
-        // k % 3 of cst, fetched two columns ahead
-        auto fetch_col = [&](int kk) {
-            const int nkk = min(wb, N - 1 - kk);
-            double* dst = cst + (kk % 3) * BAND_CREC;
-            const double* src = L + (long)kk * BAND_W * 144;
-            for (int e = tid; e < (nkk + 1) * 72 + 6; e += blockDim.x) {
-                if (e < (nkk + 1) * 72) band_cp16(dst + 2 * e, src + 2 * e);
-                else band_cp16(dst + BAND_W * 144 + 2 * (e - (nkk + 1) * 72), Y + (long)kk * 12 + 2 * (e - (nkk + 1) * 72));
-            }
-            band_cp_commit();
-        };
-        fetch_col(N - 1);
-        if (N >= 2) fetch_col(N - 2);
-        band_cp_wait_all();
-        __syncthreads();
-        for (int k = N - 1; k >= 0; k--) {
-            const int nk = min(wb, N - 1 - k);
-            const double* col = cst + (k % 3) * BAND_CREC;
-            if (k >= 2) fetch_col(k - 2);        // into the buffer column k + 1 used
-            for (int t = tid; t < 12 * nk; t += blockDim.x) {
-                int d = 1 + t / 12, r = t % 12;              // block L(k + d, k), column r
-                const double* B = col + d * 144;
-                const double* xi = xs + ((k + d) % BAND_W) * 12;
-                double acc = 0.0;
-#pragma unroll
-                for (int c = 0; c < 12; c++) acc += B[c * 12 + r] * xi[c];
-                part[(d - 1) * 12 + r] = acc;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                double t = 0.0;
-                if (lane < 12) {
-                    t = col[BAND_W * 144 + lane];
-                    for (int d = 0; d < nk; d++) t -= part[d * 12 + lane];
+        // backward on warp 0: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).
+        // The record of column k (its factor blocks, then y_k) sits in ring
+        // buffer k % 3 of cst, fetched two columns ahead
+        if (warp == 0) {
+            auto fetch_col = [&](int kk) {
+                const int nkk = min(wb, N - 1 - kk);
+                double* dst = cst + (kk % 3) * BAND_CREC;
+                const double* src = L + (long)kk * BAND_W * 144;
+                for (int e = lane; e < (nkk + 1) * 72 + 6; e += 32) {
+                    if (e < (nkk + 1) * 72) band_cp16(dst + 2 * e, src + 2 * e);
+                    else band_cp16(dst + BAND_W * 144 + 2 * (e - (nkk + 1) * 72), Y + (long)kk * 12 + 2 * (e - (nkk + 1) * 72));
                 }
+                band_cp_commit();
+            };
+            fetch_col(N - 1);
+            if (N >= 2) { fetch_col(N - 2); band_cp_wait_but_one(); } else band_cp_wait_all();
+            __syncwarp();
+            const int r = lane % 12, half = lane / 12;
+            for (int k = N - 1; k >= 0; k--) {
+                const int nk = min(wb, N - 1 - k);
+                const double* col = cst + (k % 3) * BAND_CREC;
+                if (k >= 2) fetch_col(k - 2);        // into the buffer column k + 1 used
+                // t_r = y_k[r] - sum_d (L_{k+d,k}^T x_{k+d})[r]: lanes r and r + 12 take alternate blocks d
+                double t = 0.0;
+                if (lane < 24) {
+                    double acc0 = half == 0 ? col[BAND_W * 144 + r] : 0.0, acc1 = 0.0;
+                    for (int d = 1 + half; d <= nk; d += 2) {
+                        const double* B = col + d * 144;
+                        const double* xi = xs + ((k + d) % BAND_W) * 12;
+#pragma unroll
+                        for (int c = 0; c < 12; c += 2) {
+                            acc0 = fma(-B[c * 12 + r], xi[c], acc0);
+                            acc1 = fma(-B[(c + 1) * 12 + r], xi[c + 1], acc1);
+                        }
+                    }
+                    t = acc0 + acc1;
+                }
+                t += __shfl_sync(0xffffffffu, t, (lane + 12) & 31);
                 // x_k[lane] = sum_{c >= lane} Linv[c][lane] t_c
                 double x = 0.0;
 #pragma unroll
                 for (int c = 0; c < 12; c++) {
-                    double tc = __shfl_sync(0xffffffffu, t, c);
+                    const double tc = __shfl_sync(0xffffffffu, t, c);
                     if (lane < 12 && c >= lane) x += col[c * 12 + lane] * tc;
                 }
                 if (lane < 12) { du[12L * ord[k] + lane] = x; xs[(k % BAND_W) * 12 + lane] = x; }
+                // column k - 1 (fetched during column k + 1) must have landed; the
+                // fetch issued in this column may still be in flight
+                if (k >= 2) band_cp_wait_but_one(); else band_cp_wait_all();
+                __syncwarp();
             }
-            // column k - 1 (fetched during column k + 1) must have landed; the
-            // fetch of this column may still be in flight unless it is the last
-            if (k >= 2) band_cp_wait_but_one(); else band_cp_wait_all();
-            __syncthreads();
         }
+        __syncthreads();
     }
 }
 
@@ -945,10 +1003,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
             }
         }
         CUDA_TRY(cudaMemcpyAsync(D->loff_d, D->loff_h, sizeof(long long) * nband, cudaMemcpyHostToDevice, st));
-        // window, staging, inverse diagonal factors, right-hand sides, y_k,
-        // backward partial sums and solution blocks
-        const size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 +
-                             BAND_MAX * 12 + BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * sizeof(double);
+        const size_t smem = (size_t)band_smem_doubles() * sizeof(double);
         if (!D->band_smem_set) {
             CUDA_TRY(cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             D->band_smem_set = true;

@@ -24,7 +24,7 @@ static std::vector<double> dense_solve(std::vector<double> A, std::vector<double
 }
 int main(int argc, char** argv) {
     setvbuf(stdout, nullptr, _IONBF, 0);
-    int cases[][2] = {{2, 1}, {5, 4}, {11, 8}, {17, 5}, {30, 8}};
+    int cases[][2] = {{2, 1}, {5, 4}, {9, 8}, {11, 8}, {17, 5}, {30, 8}, {40, 1}, {23, 3}};
     std::mt19937_64 rng(7);
     std::normal_distribution<double> nd(0.0, 1.0);
     double worst = 0;
@@ -51,11 +51,8 @@ int main(int argc, char** argv) {
         int cptr[2] = {0, N}, cbw[1] = {wb}; long long loff[1] = {0};
         std::vector<double> Lg((size_t)N * BAND_W * 144 + 12 * N, 0.0), du(n, 0.0);
         int status = 0;
-        // the kernel's shared-memory layout (as dense.cu sizes it): window,
-        // staging, inverse factors, right-hand sides, y_k, partial sums,
-        // solution blocks, staged right-hand sides, backward records
-        size_t smem = ((size_t)BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_MAX * 12 +
-                       BAND_W * 12 + 2 * 12 + 3 * BAND_CREC) * 8;
+        // the kernel's shared-memory size, as the solver launches it
+        size_t smem = (size_t)band_smem_doubles() * 8;
         const long long ltot = (long long)N * BAND_W;
         launch(1, BAND_THREADS, smem, [&] { k_band_solve(1, cptr, order.data(), cbw, loff, Ab.data(), ltot, g.data(), Lg.data(), du.data(), &status); });
         auto ref = dense_solve(M, g, n);

@@ -25,7 +25,7 @@ def _kernel_source():
     k = k.replace("extern __shared__ __align__(16) unsigned char smem_raw[];", "unsigned char* smem_raw = g_dyn_smem;")
     k = k.replace("__shared__ unsigned char tri_a", "static unsigned char tri_a").replace("__shared__ int ord[", "static int ord[")
     # the gather kernel reads the block CSR of the engine: not needed here
-    return k[:k.index("template <class TV>")] + k[k.index("// Warp-wide: Cholesky factor"):]
+    return k[:k.index("template <class TV>")] + k[k.index("// Warp-wide Cholesky factorization and inversion"):]
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
