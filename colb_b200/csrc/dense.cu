@@ -284,6 +284,11 @@ DV void band_cp_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memo
 // shared-memory writes to the waiting threads, or arrive and wait
 DV void band_bar_arrive(int id, int n) { asm volatile("barrier.arrive %0, %1;" :: "r"(id), "r"(n) : "memory"); }
 DV void band_bar_sync(int id, int n) { asm volatile("barrier.sync %0, %1;" :: "r"(id), "r"(n) : "memory"); }
+// cluster barrier in two halves: arrive (release: this thread's earlier
+// writes, global memory included, become visible to the cluster) and wait
+// (acquire); every thread of the cluster arrives once per phase
+DV void band_cluster_arrive() { asm volatile("barrier.cluster.arrive.release;" ::: "memory"); }
+DV void band_cluster_wait() { asm volatile("barrier.cluster.wait.acquire;" ::: "memory"); }
 
 // A component whose bodies, in reverse Cuthill-McKee order, couple only
 // bodies at most BAND_MAX apart is a block band matrix: its Cholesky factor
@@ -321,16 +326,21 @@ constexpr int BAND_THREADS = 256;
 // bank 0, and tiles of different blocks read by one warp would conflict)
 constexpr int BAND_BLK = 146;
 constexpr int BAND_CREC = BAND_W * 144 + 12;   // backward record: factor column blocks, then y_k
-// dynamic shared memory of k_band_solve in doubles: window, staged block
-// rows, inverse diagonal factors, right-hand sides, y_k, solution blocks,
-// staged right-hand sides, backward records
-constexpr int band_smem_doubles() {
-    return BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_W * 12 + 2 * 12 +
-           3 * BAND_CREC;
-}
-
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
 constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
+// dynamic shared memory of k_band_solve in doubles: window, staged block
+// rows, inverse diagonal factors, right-hand sides, y_k, solution blocks,
+// staged right-hand sides, backward records, then the body order (ints)
+// and the block-pair tables (bytes)
+constexpr int band_smem_doubles() {
+    return BAND_W * BAND_W * BAND_BLK + 2 * BAND_W * 144 + 2 * 144 + BAND_W * 12 + 12 + BAND_W * 12 + 2 * 12 +
+           3 * BAND_CREC + BAND_ORD_MAX / 2 + (BAND_MAX * (BAND_MAX + 1) + 7) / 8;
+}
+// a component of n bodies and body bandwidth wb is split between the two
+// CTAs of its cluster at position m = (n - wb) / 2 when both halves keep at
+// least wb / 2 + 6 block columns; -1 when it is factored by one CTA
+inline int band_split_point(int n, int wb) { return n >= 2 * wb + 12 ? (n - wb) / 2 : -1; }
+
 
 // 1/sqrt(d): the single-precision estimate r0 (relative error below 2^-22)
 // refined by one third-order Householder step.  With e = 1 - d r0^2,
@@ -440,8 +450,21 @@ DV void band_panel_row(double* R, const double* Li, int half, bool act) {
     __syncwarp();
 }
 
+// One job per cluster of two CTAs.  A job is a band component (sub-component
+// ct) factored by CTA 0 alone, or a large one split in two: ct holds its
+// bodies [0, m + wb) in order, cb the bodies [m, N) in reverse order, and
+// S = [m, m + wb) separates [0, m) from [m + wb, N) (the band couples bodies
+// at most wb apart).  CTA 0 eliminates [0, m) while CTA 1 eliminates
+// [m + wb, N) from the far end; each leaves S in its window with its own
+// Schur update applied.  After a cluster barrier CTA 0 adds CTA 1's update
+// (S = W0 + W1 - A_SS, right-hand sides likewise), factors and solves S,
+// and signals the solution at a second cluster barrier; then both CTAs run
+// their backward halves.  The dependent chain shrinks from N block columns
+// each way to about (N - wb) / 2 + wb.  jobs holds (ct, cb, m) per job,
+// cb = -1 for an unsplit component (m is then its size).
 // one CTA per SM (its shared memory allows no second), so the register cap is set for one
-__global__ void __launch_bounds__(BAND_THREADS, 1) k_band_solve(int ncomp, const int* __restrict__ cptr,
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(BAND_THREADS, 1)
+k_band_solve(int njobs, const int* __restrict__ jobs, const int* __restrict__ cptr,
         const int* __restrict__ order, const int* __restrict__ cbw, const long long* __restrict__ loff,
         const double* __restrict__ Ab, long long ltot, const double* __restrict__ g, double* Lg, double* du,
         int* status) {
@@ -454,16 +477,29 @@ __global__ void __launch_bounds__(BAND_THREADS, 1) k_band_solve(int ncomp, const
     double* xs = ybuf + 12;                                   // [BAND_W][12] latest solution blocks (backward)
     double* gst = xs + BAND_W * 12;                           // [2][12] right-hand side of each staged block row
     double* cst = gst + 2 * 12;                               // [3][BAND_CREC] backward factor columns and y_k
-    __shared__ unsigned char tri_a[BAND_MAX * (BAND_MAX + 1) / 2], tri_b[BAND_MAX * (BAND_MAX + 1) / 2];
-    __shared__ int ord[BAND_ORD_MAX];
+    int* ord = (int*)(cst + 3 * BAND_CREC);                   // [BAND_ORD_MAX] bodies of the sub-component
+    unsigned char* tri_a = (unsigned char*)(ord + BAND_ORD_MAX);   // block pair p -> (a, b), b <= a
+    unsigned char* tri_b = tri_a + BAND_MAX * (BAND_MAX + 1) / 2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int t1 = tid - 32, n1 = blockDim.x - 32;            // thread index among warps 1..7
+    const int crank = blockIdx.x & 1;                         // rank in the cluster
     if (tid < BAND_MAX * (BAND_MAX + 1) / 2) {
         int a = 0; while ((a + 1) * (a + 2) / 2 <= tid) a++;
         tri_a[tid] = (unsigned char)a; tri_b[tid] = (unsigned char)(tid - a * (a + 1) / 2);
     }
-    for (int cc = blockIdx.x; cc < ncomp; cc += gridDim.x) {
+    for (int jb = blockIdx.x >> 1; jb < njobs; jb += gridDim.x >> 1) {
+        const int ct = jobs[3 * jb], cb = jobs[3 * jb + 1], msplit = jobs[3 * jb + 2];
+        const bool split = cb >= 0;
+        if (crank == 1 && !split) {
+            // nothing to factor: keep the cluster barriers in step with CTA 0
+            band_cluster_arrive(); band_cluster_wait();
+            band_cluster_arrive(); band_cluster_wait();
+            continue;
+        }
+        const int cc = crank == 0 ? ct : cb;
         const int N = cptr[cc + 1] - cptr[cc], wb = cbw[cc];
+        // columns this CTA eliminates before the merge
+        const int ncol1 = !split ? N : (crank == 0 ? msplit : N - wb);
         for (int e = tid; e < N; e += blockDim.x) ord[e] = order[cptr[cc] + e];
         double* L = Lg + loff[cc] * 144;                      // Linv_k at (k BAND_W), L(k + d, k) at (k BAND_W + d)
         double* Y = Lg + ltot * 144 + (loff[cc] / BAND_W) * 12;   // y_k at k * 12
@@ -496,144 +532,148 @@ __global__ void __launch_bounds__(BAND_THREADS, 1) k_band_solve(int ncomp, const
             }
             band_cp_commit();
         };
-        if (warp > 0 && wb + 1 < N) fetch_row(wb + 1);
-        __syncthreads();
-        if (warp == 0) {
-            const double* D = slot(0, 0);
+        // warp 0: factor and invert the diagonal block in slot(k, k) into linv[k & 1]
+        auto factor_diag = [&](int k) {
+            const double* D = slot(k, k);
             double a[12];
 #pragma unroll
             for (int c = 0; c < 12; c++) a[c] = lane < 12 ? D[lane * 12 + c] : 0.0;
             band_chol_inverse_rows(a, status);
             if (lane < 12) {
 #pragma unroll
-                for (int c = 0; c < 12; c++) linv[lane * 12 + c] = a[c];
+                for (int c = 0; c < 12; c++) linv[(k & 1) * 144 + lane * 12 + c] = a[c];
             }
-        }
-        __syncthreads();
-        // with a body bandwidth wb >= 1 (a connected component of two or more
-        // bodies), every column but the last has nk >= 1 blocks below the diagonal
-        for (int k = 0; k < N; k++) {
-            const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
-            const double* Li = linv + (k & 1) * 144;
-            if (warp == 0) {
-                // panel block row k + 1 (lanes r and r + 12 share row r), signalled to warps 1..7
-                const int r = lane % 12, half = lane / 12;
-                double* P = slot(k + 1, k);
-                if (nk > 0) band_panel_row(P + r * 12, Li, half, lane < 24);
-                band_bar_arrive(1, blockDim.x);
-                if (nk > 0) {
-                    // row r of A_{k+1,k+1} - L_{k+1,k} L_{k+1,k}^T: lane r forms entries 0..5,
-                    // lane r + 12 entries 6..11 and passes them to lane r
-                    const double* Dk = slot(k + 1, k + 1);
-                    double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                    if (lane < 24) {
-                        double lr[12];
+        };
+        // block columns k0..k1-1; Linv_k0 is in linv[k0 & 1].  When k1 < N
+        // the last column leaves the next diagonal block unfactored, its
+        // update applied by warps 1..7 like every other block pair.
+        auto columns = [&](int k0, int k1) {
+            for (int k = k0; k < k1; k++) {
+                const int nk = min(wb, N - 1 - k);               // blocks below the diagonal in this column
+                const bool factor_next = k + 1 < k1;
+                const double* Li = linv + (k & 1) * 144;
+                if (warp == 0) {
+                    // panel block row k + 1 (lanes r and r + 12 share row r), signalled to warps 1..7
+                    const int r = lane % 12, half = lane / 12;
+                    double* P = slot(k + 1, k);
+                    if (nk > 0) band_panel_row(P + r * 12, Li, half, lane < 24);
+                    band_bar_arrive(1, blockDim.x);
+                    if (nk > 0 && factor_next) {
+                        // row r of A_{k+1,k+1} - L_{k+1,k} L_{k+1,k}^T: lane r forms entries 0..5,
+                        // lane r + 12 entries 6..11 and passes them to lane r
+                        const double* Dk = slot(k + 1, k + 1);
+                        double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                        if (lane < 24) {
+                            double lr[12];
 #pragma unroll
-                        for (int s = 0; s < 12; s++) lr[s] = P[r * 12 + s];
+                            for (int s = 0; s < 12; s++) lr[s] = P[r * 12 + s];
+#pragma unroll
+                            for (int c6 = 0; c6 < 6; c6++) {
+                                const int c = half * 6 + c6;
+                                double acc0 = Dk[r * 12 + c], acc1 = 0.0;
+#pragma unroll
+                                for (int s = 0; s < 12; s += 2) {
+                                    acc0 = fma(-lr[s], P[c * 12 + s], acc0);
+                                    acc1 = fma(-lr[s + 1], P[c * 12 + s + 1], acc1);
+                                }
+                                h[c6] = acc0 + acc1;
+                            }
+                        }
+                        double a[12];
 #pragma unroll
                         for (int c6 = 0; c6 < 6; c6++) {
-                            const int c = half * 6 + c6;
-                            double acc0 = Dk[r * 12 + c], acc1 = 0.0;
+                            const double o = __shfl_sync(0xffffffffu, h[c6], (lane + 12) & 31);
+                            a[c6] = lane < 12 ? h[c6] : 0.0;
+                            a[6 + c6] = lane < 12 ? o : 0.0;
+                        }
+                        band_chol_inverse_rows(a, status);
+                        if (lane < 12) {
+                            double* Ln = linv + ((k + 1) & 1) * 144;
 #pragma unroll
-                            for (int s = 0; s < 12; s += 2) {
-                                acc0 = fma(-lr[s], P[c * 12 + s], acc0);
-                                acc1 = fma(-lr[s + 1], P[c * 12 + s + 1], acc1);
-                            }
-                            h[c6] = acc0 + acc1;
+                            for (int c = 0; c < 12; c++) Ln[lane * 12 + c] = a[c];
                         }
                     }
-                    double a[12];
+                } else {
+                    if (warp < 7) {
+                        // panel rows of blocks k + 2 .. k + nk, two adjacent lanes per row
+                        const int q = 12 + (t1 >> 1);
+                        const bool act = q < 12 * nk;
+                        band_panel_row(act ? slot(k + 1 + q / 12, k) + (q % 12) * 12 : win, Li, t1 & 1, act);
+                    } else if (lane < 12) {
+                        const double* rk = rhs + (k % BAND_W) * 12;
+                        double y = 0.0;
 #pragma unroll
-                    for (int c6 = 0; c6 < 6; c6++) {
-                        const double o = __shfl_sync(0xffffffffu, h[c6], (lane + 12) & 31);
-                        a[c6] = lane < 12 ? h[c6] : 0.0;
-                        a[6 + c6] = lane < 12 ? o : 0.0;
+                        for (int s = 0; s < 12; s++) if (s <= lane) y += Li[lane * 12 + s] * rk[s];
+                        ybuf[lane] = y;
+                        Y[(long)k * 12 + lane] = y;
                     }
-                    band_chol_inverse_rows(a, status);
-                    if (lane < 12) {
-                        double* Ln = linv + ((k + 1) & 1) * 144;
+                    band_cp_wait_all();              // this thread's copies of the staged block row
+                    band_bar_sync(1, blockDim.x);    // panel (warp 0's row included), y_k and the staged row are there
+                    // A_ij -= L_ik L_jk^T over the window in 3 x 4 tiles (12 per
+                    // block pair); pair 0, (k+1, k+1), is warp 0's unless it stays unfactored
+                    const int npair = nk * (nk + 1) / 2;
+                    for (int e = t1 + (factor_next ? 12 : 0); e < npair * 12; e += n1) {
+                        int p = e / 12, tile = e % 12;
+                        int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
+                        int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
+                        const double* Lia = slot(i, k) + r0t * 12;
+                        const double* Ljb = slot(j, k) + c0t * 12;
+                        double acc[3][4] = {};
 #pragma unroll
-                        for (int c = 0; c < 12; c++) Ln[lane * 12 + c] = a[c];
-                    }
-                }
-            } else {
-                if (warp < 7) {
-                    // panel rows of blocks k + 2 .. k + nk, two adjacent lanes per row
-                    const int q = 12 + (t1 >> 1);
-                    const bool act = q < 12 * nk;
-                    band_panel_row(act ? slot(k + 1 + q / 12, k) + (q % 12) * 12 : win, Li, t1 & 1, act);
-                } else if (lane < 12) {
-                    const double* rk = rhs + (k % BAND_W) * 12;
-                    double y = 0.0;
+                        for (int s = 0; s < 12; s++) {
+                            double li[3], lj[4];
 #pragma unroll
-                    for (int s = 0; s < 12; s++) if (s <= lane) y += Li[lane * 12 + s] * rk[s];
-                    ybuf[lane] = y;
-                    Y[(long)k * 12 + lane] = y;
-                }
-                band_cp_wait_all();              // this thread's copies of the staged block row
-                band_bar_sync(1, blockDim.x);    // panel (warp 0's row included), y_k and the staged row are there
-                // A_ij -= L_ik L_jk^T over the window in 3 x 4 tiles (12 per
-                // block pair); pair 0, (k+1, k+1), is warp 0's
-                const int npair = nk * (nk + 1) / 2;
-                for (int e = t1 + 12; e < npair * 12; e += n1) {
-                    int p = e / 12, tile = e % 12;
-                    int i = k + 1 + tri_a[p], j = k + 1 + tri_b[p];
-                    int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
-                    const double* Lia = slot(i, k) + r0t * 12;
-                    const double* Ljb = slot(j, k) + c0t * 12;
-                    double acc[3][4] = {};
+                            for (int a2 = 0; a2 < 3; a2++) li[a2] = Lia[a2 * 12 + s];
 #pragma unroll
-                    for (int s = 0; s < 12; s++) {
-                        double li[3], lj[4];
+                            for (int b2 = 0; b2 < 4; b2++) lj[b2] = Ljb[b2 * 12 + s];
 #pragma unroll
-                        for (int a2 = 0; a2 < 3; a2++) li[a2] = Lia[a2 * 12 + s];
+                            for (int a2 = 0; a2 < 3; a2++)
 #pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) lj[b2] = Ljb[b2 * 12 + s];
+                                for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
+                        }
+                        double* Aij = slot(i, j);
 #pragma unroll
                         for (int a2 = 0; a2 < 3; a2++)
 #pragma unroll
-                            for (int b2 = 0; b2 < 4; b2++) acc[a2][b2] += li[a2] * lj[b2];
+                            for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
                     }
-                    double* Aij = slot(i, j);
+                    // rhs_i -= L_ik y_k
+                    for (int t = t1; t < 12 * nk; t += n1) {
+                        int i = k + 1 + t / 12, r = t % 12;
+                        const double* R = slot(i, k) + r * 12;
+                        double acc = 0.0;
 #pragma unroll
-                    for (int a2 = 0; a2 < 3; a2++)
-#pragma unroll
-                        for (int b2 = 0; b2 < 4; b2++) Aij[(r0t + a2) * 12 + c0t + b2] -= acc[a2][b2];
-                }
-                // rhs_i -= L_ik y_k
-                for (int t = t1; t < 12 * nk; t += n1) {
-                    int i = k + 1 + t / 12, r = t % 12;
-                    const double* R = slot(i, k) + r * 12;
-                    double acc = 0.0;
-#pragma unroll
-                    for (int c = 0; c < 12; c++) acc += R[c] * ybuf[c];
-                    rhs[(i % BAND_W) * 12 + r] -= acc;
-                }
-                // factor column k to global: Linv_k, then L(k + d, k)
-                for (int e = t1; e < (nk + 1) * 144; e += n1) {
-                    int d = e / 144, q = e % 144;
-                    L[((long)k * BAND_W + d) * 144 + q] = d == 0 ? Li[q] : slot(k + d, k)[q];
-                }
-                // block row k + 1 + wb enters the window (staged during the
-                // previous column; its ring row is that of row k, free now),
-                // and row k + 2 + wb is fetched
-                const int m1 = k + 1 + wb, m2 = k + 2 + wb;
-                if (m1 < N) {
-                    const double* src = stage + (m1 & 1) * BAND_W * 144;
-                    for (int e = t1; e < (wb + 1) * 144; e += n1) {
-                        int q = e / 144, x = e % 144;             // block q: column k + 1 + q
-                        slot(m1, k + 1 + q)[x] = src[e];
+                        for (int c = 0; c < 12; c++) acc += R[c] * ybuf[c];
+                        rhs[(i % BAND_W) * 12 + r] -= acc;
                     }
-                    if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = gst[(m1 & 1) * 12 + t1];
+                    // factor column k to global: Linv_k, then L(k + d, k)
+                    for (int e = t1; e < (nk + 1) * 144; e += n1) {
+                        int d = e / 144, q = e % 144;
+                        L[((long)k * BAND_W + d) * 144 + q] = d == 0 ? Li[q] : slot(k + d, k)[q];
+                    }
+                    // block row k + 1 + wb enters the window (staged during the
+                    // previous column; its ring row is that of row k, free now),
+                    // and row k + 2 + wb is fetched
+                    const int m1 = k + 1 + wb, m2 = k + 2 + wb;
+                    if (m1 < N) {
+                        const double* src = stage + (m1 & 1) * BAND_W * 144;
+                        for (int e = t1; e < (wb + 1) * 144; e += n1) {
+                            int q = e / 144, x = e % 144;             // block q: column k + 1 + q
+                            slot(m1, k + 1 + q)[x] = src[e];
+                        }
+                        if (t1 < 12) rhs[(m1 % BAND_W) * 12 + t1] = gst[(m1 & 1) * 12 + t1];
+                    }
+                    if (m2 < N) fetch_row(m2);
                 }
-                if (m2 < N) fetch_row(m2);
+                __syncthreads();
             }
-            __syncthreads();
-        }
-        // backward on warp 0: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}).
-        // The record of column k (its factor blocks, then y_k) sits in ring
-        // buffer k % 3 of cst, fetched two columns ahead
-        if (warp == 0) {
+        };
+        // warp 0: x_k = Linv_k^T (y_k - sum_d L_{k+d,k}^T x_{k+d}) for
+        // k = kfirst down to 0, the solution blocks above kfirst already in
+        // xs.  The record of column k (its factor blocks, then y_k) sits in
+        // ring buffer k % 3 of cst, fetched two columns ahead.  After column
+        // kcall the callback runs (once).
+        auto backward = [&](int kfirst, int kcall, auto&& callback) {
             auto fetch_col = [&](int kk) {
                 const int nkk = min(wb, N - 1 - kk);
                 double* dst = cst + (kk % 3) * BAND_CREC;
@@ -644,11 +684,11 @@ __global__ void __launch_bounds__(BAND_THREADS, 1) k_band_solve(int ncomp, const
                 }
                 band_cp_commit();
             };
-            fetch_col(N - 1);
-            if (N >= 2) { fetch_col(N - 2); band_cp_wait_but_one(); } else band_cp_wait_all();
+            fetch_col(kfirst);
+            if (kfirst >= 1) { fetch_col(kfirst - 1); band_cp_wait_but_one(); } else band_cp_wait_all();
             __syncwarp();
             const int r = lane % 12, half = lane / 12;
-            for (int k = N - 1; k >= 0; k--) {
+            for (int k = kfirst; k >= 0; k--) {
                 const int nk = min(wb, N - 1 - k);
                 const double* col = cst + (k % 3) * BAND_CREC;
                 if (k >= 2) fetch_col(k - 2);        // into the buffer column k + 1 used
@@ -676,11 +716,77 @@ __global__ void __launch_bounds__(BAND_THREADS, 1) k_band_solve(int ncomp, const
                     if (lane < 12 && c >= lane) x += col[c * 12 + lane] * tc;
                 }
                 if (lane < 12) { du[12L * ord[k] + lane] = x; xs[(k % BAND_W) * 12 + lane] = x; }
+                if (k == kcall) callback();
                 // column k - 1 (fetched during column k + 1) must have landed; the
                 // fetch issued in this column may still be in flight
                 if (k >= 2) band_cp_wait_but_one(); else band_cp_wait_all();
                 __syncwarp();
             }
+        };
+        auto nothing = [] {};
+
+        if (warp > 0 && wb + 1 < N) fetch_row(wb + 1);
+        __syncthreads();
+        if (warp == 0) factor_diag(0);
+        __syncthreads();
+        // with a body bandwidth wb >= 1 (a connected component of two or more
+        // bodies), every column but the last has nk >= 1 blocks below the diagonal
+        columns(0, ncol1);
+        if (!split) {
+            if (warp == 0) backward(N - 1, -1, nothing);
+            band_cluster_arrive(); band_cluster_wait();
+            band_cluster_arrive(); band_cluster_wait();
+        } else if (crank == 1) {
+            // hand S (positions ncol1..N-1, the separator in reverse order)
+            // to CTA 0 in this sub-component's unused factor slots: block
+            // (p, q) at (p BAND_W + p - q), its right-hand side at Y + 12 p
+            for (int e = tid; e < wb * BAND_W * 144; e += blockDim.x) {
+                const int p = ncol1 + e / (BAND_W * 144), d = (e / 144) % BAND_W, x = e % 144;
+                if (p - d >= ncol1) L[((long)p * BAND_W + d) * 144 + x] = slot(p, p - d)[x];
+            }
+            for (int e = tid; e < wb * 12; e += blockDim.x) Y[(long)(ncol1 + e / 12) * 12 + e % 12] = rhs[((ncol1 + e / 12) % BAND_W) * 12 + e % 12];
+            __threadfence();
+            band_cluster_arrive(); band_cluster_wait();       // S handed over
+            band_cluster_arrive(); band_cluster_wait();       // S solved by CTA 0
+            if (warp == 0) {
+                // x of the separator from du, then the backward half
+                for (int e = lane; e < wb * 12; e += 32) {
+                    const int p = ncol1 + e / 12;
+                    xs[(p % BAND_W) * 12 + e % 12] = __ldcg(du + 12L * ord[p] + e % 12);
+                }
+                __syncwarp();
+                backward(ncol1 - 1, -1, nothing);
+            }
+        } else {
+            band_cluster_arrive(); band_cluster_wait();       // CTA 1's half of S is in global memory
+            // S = W0 + W1 - A_SS: window row i (forward position) takes block
+            // (i, j) of CTA 1 as its transposed reverse block (pj, pi),
+            // pi = Nt - 1 - i with Nt = m + N1 the component size
+            const int ncb = cptr[cb + 1] - cptr[cb];
+            const double* L1 = Lg + loff[cb] * 144;
+            const double* Y1 = Lg + ltot * 144 + (loff[cb] / BAND_W) * 12;
+            const int nt1 = msplit + ncb - 1;                 // forward position i <-> reverse position nt1 - i
+            for (int e = tid; e < wb * wb * 144; e += blockDim.x) {
+                const int i = msplit + e / (wb * 144), j = msplit + (e / 144) % wb, x = e % 144;
+                if (j > i) continue;
+                const int rr = x / 12, c = x % 12, pi = nt1 - i, pj = nt1 - j;
+                const double w1 = __ldcg(L1 + ((long)pj * BAND_W + (pj - pi)) * 144 + c * 12 + rr);
+                slot(i, j)[x] += w1 - A[((long)i * BAND_W + (i - j)) * 144 + x];
+            }
+            for (int e = tid; e < wb * 12; e += blockDim.x) {
+                const int i = msplit + e / 12, rr = e % 12;
+                rhs[(i % BAND_W) * 12 + rr] += __ldcg(Y1 + (long)(nt1 - i) * 12 + rr) - g[12L * ord[i] + rr];
+            }
+            __syncthreads();
+            if (warp == 0) factor_diag(msplit);
+            __syncthreads();
+            columns(msplit, N);
+            if (warp == 0) {
+                backward(N - 1, msplit, [&] { __threadfence(); band_cluster_arrive(); });
+            } else {
+                band_cluster_arrive();
+            }
+            band_cluster_wait();
         }
         __syncthreads();
     }
@@ -736,7 +842,9 @@ static int dense_init(Engine* E) {
     E->dense_state = D;
     if (cusolverDnCreate(&D->h) != CUSOLVER_STATUS_SUCCESS) return E->fail(ABD_ERR_CUDA, "cusolverDnCreate");
     cusolverDnSetStream(D->h, E->stream);
-    size_t ni = 8 * (size_t)E->nb + 16;
+    // component maps, small-component lists, band sub-components (a split
+    // component's separator appears in both halves) and band jobs
+    size_t ni = 10 * (size_t)E->nb + 16;
     if (cudaMalloc(&D->imap_d, sizeof(int) * ni) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc maps");
     if (cudaMallocHost(&D->imap_h, sizeof(int) * ni) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMallocHost maps");
     if (cudaMalloc(&D->loff_d, sizeof(long long) * (E->nb + 1)) != cudaSuccess) return E->fail(ABD_ERR_CUDA, "cudaMalloc band offsets");
@@ -905,10 +1013,19 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     // ones (cuSOLVER)
     D->root.assign(nb, -1);
     D->bmap.assign(nb, -1);
-    std::vector<int> small_root, large_n, band_cptr(1, 0), band_bw, band_order, ord;
+    std::vector<int> small_root, large_n, band_cptr(1, 0), band_bw, band_order, ord, band_jobs;
     std::vector<long long> large_off, large_rhs;
     long long aoff = 0, roff = 0, lblocks = 0;
-    int nmax_large = 0, nmax_small = 0, small_bodies = 0, nband = 0;
+    int nmax_large = 0, nmax_small = 0, small_bodies = 0, nband = 0, ncomp_band = 0;
+    // a band sub-component: bodies in factor order, body bandwidth
+    auto band_sub = [&](const int* bodies, int len, int bw) {
+        D->loff_h[nband] = lblocks;
+        lblocks += (long long)len * BAND_W;
+        band_order.insert(band_order.end(), bodies, bodies + len);
+        band_cptr.push_back((int)band_order.size());
+        band_bw.push_back(bw);
+        return nband++;
+    };
     for (int b = 0; b < nb; b++) {
         int r = find(b), sz = D->size[r];
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
@@ -920,14 +1037,19 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         if (D->root[r] == -1 && projected && !E->mixed &&
             (sz <= BAND_PREFER_MAX || (int)large_n.size() >= MAX_LARGE_COMPONENTS / 2)) {
             int bw = rcm(r, ord);
-            if (bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
-                D->root[r] = -10 - nband;                 // marks a band component
-                D->loff_h[nband] = lblocks;
-                lblocks += (long long)sz * BAND_W;
-                band_order.insert(band_order.end(), ord.begin(), ord.end());
-                band_cptr.push_back((int)band_order.size());
-                band_bw.push_back(bw);
-                nband++;
+            if (bw >= 1 && bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
+                D->root[r] = -10 - ncomp_band++;          // marks a band component
+                const int m = band_split_point(sz, bw);
+                if (m > 0) {
+                    // bodies [0, m + bw) forward, [m, sz) from the far end
+                    const int ct = band_sub(ord.data(), m + bw, bw);
+                    std::vector<int> rev(ord.rbegin(), ord.rend() - m);
+                    const int cb = band_sub(rev.data(), sz - m, bw);
+                    band_jobs.insert(band_jobs.end(), {ct, cb, m});
+                } else {
+                    const int ct = band_sub(ord.data(), sz, bw);
+                    band_jobs.insert(band_jobs.end(), {ct, -1, sz});
+                }
             }
         }
         if (D->root[r] <= -10) { D->bmap[b] = -3; continue; }
@@ -949,7 +1071,7 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         else D->bmap[b] = D->root[r];
     }
     const int nsmall = (int)small_root.size(), nlarge = (int)large_n.size();
-    E->comp_band += nband; E->comp_small += nsmall; E->comp_large += nlarge;
+    E->comp_band += ncomp_band; E->comp_small += nsmall; E->comp_large += nlarge;
 
     if (aoff * (long long)sizeof(T) > (4LL << 30)) { *fallback = 1; E->krylov_fallbacks++; return ABD_OK; }
     // local body index inside its component (body order) and the small
@@ -982,7 +1104,10 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
     int* h_pcomp = h_bord + band_order.size();
     for (int c = 0; c < nband; c++)
         for (int q = band_cptr[c]; q < band_cptr[c + 1]; q++) h_pcomp[q] = c;
-    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies + 2 * (size_t)nband + 1 + 2 * band_order.size();
+    int* h_jobs = h_pcomp + band_order.size();
+    for (size_t i = 0; i < band_jobs.size(); i++) h_jobs[i] = band_jobs[i];
+    const size_t nints = 2 * (size_t)nb + nsmall + 1 + small_bodies + 2 * (size_t)nband + 1 + 2 * band_order.size() +
+                         band_jobs.size();
     CUDA_TRY(cudaMemcpyAsync(D->imap_d, h, sizeof(int) * nints, cudaMemcpyHostToDevice, st));
     const int* d_bmap = D->imap_d; const int* d_blocal = D->imap_d + nb;
     const int* d_sptr = D->imap_d + 2 * nb; const int* d_sbody = d_sptr + nsmall + 1;
@@ -1009,13 +1134,16 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
             D->band_smem_set = true;
         }
         const int* d_pcomp = d_bord + band_order.size();
-        const int npos = (int)band_order.size();
+        const int* d_jobs = d_pcomp + band_order.size();
+        const int npos = (int)band_order.size(), njobs = (int)band_jobs.size() / 3;
         k_band_gather<T><<<grid_for(32L * npos * BAND_W), 256, 0, st>>>(npos, d_pcomp, d_bcptr, d_bord, d_bbw, D->loff_d,
                                                                        E->row_ptr, E->bcol, (const T*)E->vals, (double*)D->Ab);
         E->launches++;
         int ph = phase_begin(E, PH_BAND);
-        k_band_solve<<<nband, BAND_THREADS, smem, st>>>(nband, d_bcptr, d_bord, d_bbw, D->loff_d, (const double*)D->Ab,
-                                                        lblocks, E->g, (double*)D->Lg, E->du, D->info);
+        // one cluster of two CTAs per job
+        k_band_solve<<<2 * njobs, BAND_THREADS, smem, st>>>(njobs, d_jobs, d_bcptr, d_bord, d_bbw, D->loff_d,
+                                                            (const double*)D->Ab, lblocks, E->g, (double*)D->Lg, E->du,
+                                                            D->info);
         // per component: band blocks read, factor written and read back,
         // g read, y and du written and read
         double bytes = 0;
