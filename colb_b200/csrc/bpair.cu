@@ -46,14 +46,17 @@ DV void vbox(const double* x, const double* p, int v, float pad, float4& lo, flo
                      __fadd_ru(__double2float_ru(fmax(a2, b2)), pad), 0.f);
 }
 
-// 1. body boxes: one warp per body over its vertices
+// 1. body boxes: one warp per body over its vertices; with vlo/vhi given,
+// every vertex's box is kept too (the primitive boxes of the pair tests are
+// the min/max over their vertices' boxes, exact in float)
 __global__ void k_body_boxes(int nb, const int* __restrict__ vbeg, const double* __restrict__ x, const double* __restrict__ p,
-                             float pad, float4* blo, float4* bhi) {
+                             float pad, float4* blo, float4* bhi, float4* vlo = nullptr, float4* vhi = nullptr) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     for (int b = warp; b < nb; b += (gridDim.x * blockDim.x) >> 5) {
         float4 lo = make_float4(3e38f, 3e38f, 3e38f, 0.f), hi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
         for (int v = vbeg[b] + lane; v < vbeg[b+1]; v += 32) {
             float4 l, h; vbox(x, p, v, pad, l, h);
+            if (vlo) { vlo[v] = l; vhi[v] = h; }
             lo = fmin4(lo, l); hi = fmax4(hi, h);
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -102,6 +105,7 @@ DV int stage(int begin, int end, float4 rlo, float4 rhi, BoxFn box, int* idx, fl
 
 struct BpArgs {
     Geo G; const double* p; const float* pmag;
+    const float4* vlo; const float4* vhi;          // per-vertex swept boxes of this build
     const int* ebeg; const int* tbeg; const int* vbeg;
     const float4* blo; const float4* bhi;
     float pad; double lim; double filt; int mode;   // mode 0 swept (Lipschitz, lim), 1 detect (predicate, filt)
@@ -154,17 +158,18 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp_prims(const int2* __restrict_
         int2 bp = bpairs[q];
         int ba = bp.x, bb = bp.y;
         float4 rlo = fmax4(A.blo[ba], A.blo[bb]), rhi = fmin4(A.bhi[ba], A.bhi[bb]);
+        const float4* __restrict__ vlo = A.vlo;
+        const float4* __restrict__ vhi = A.vhi;
         auto ebox = [&](int e, float4& l, float4& h) {
             int2 ed = G.edges[e];
-            float4 l0, h0, l1, h1; vbox(G.x, A.p, ed.x, pad, l0, h0); vbox(G.x, A.p, ed.y, pad, l1, h1);
-            l = fmin4(l0, l1); h = fmax4(h0, h1);
+            l = fmin4(__ldg(vlo + ed.x), __ldg(vlo + ed.y)); h = fmax4(__ldg(vhi + ed.x), __ldg(vhi + ed.y));
         };
         auto tbox = [&](int t, float4& l, float4& h) {
-            float4 l0, h0, l1, h1, l2, h2;
-            vbox(G.x, A.p, G.tris[3*t], pad, l0, h0); vbox(G.x, A.p, G.tris[3*t+1], pad, l1, h1); vbox(G.x, A.p, G.tris[3*t+2], pad, l2, h2);
-            l = fmin4(l0, fmin4(l1, l2)); h = fmax4(h0, fmax4(h1, h2));
+            const int v0 = G.tris[3*t], v1 = G.tris[3*t+1], v2 = G.tris[3*t+2];
+            l = fmin4(__ldg(vlo + v0), fmin4(__ldg(vlo + v1), __ldg(vlo + v2)));
+            h = fmax4(__ldg(vhi + v0), fmax4(__ldg(vhi + v1), __ldg(vhi + v2)));
         };
-        auto pbox = [&](int v, float4& l, float4& h) { vbox(G.x, A.p, v, pad, l, h); };
+        auto pbox = [&](int v, float4& l, float4& h) { l = __ldg(vlo + v); h = __ldg(vhi + v); };
         // ---- edge-edge
         if (A.do_ee) {
             for (int a0 = A.ebeg[ba]; a0 < A.ebeg[ba+1]; a0 += BP_CHUNK) {
@@ -172,13 +177,17 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp_prims(const int2* __restrict_
                 if (na == 0) continue;
                 for (int b0 = A.ebeg[bb]; b0 < A.ebeg[bb+1]; b0 += BP_CHUNK) {
                     int nbb = stage(b0, min(b0 + BP_CHUNK, A.ebeg[bb+1]), rlo, rhi, ebox, bidx, blo, bhi, &sb);
-                    for (long t = threadIdx.x; t < (long)na * nbb; t += blockDim.x) {
-                        int ia = (int)(t / nbb), ib = (int)(t % nbb);
-                        int i = aidx[ia], j = bidx[ib];
-                        if (ba == bb && i >= j) continue;
-                        if (!overlap(alo[ia], ahi[ia], blo[ib], bhi[ib])) continue;
-                        int lo_ = min(i, j), hi_ = max(i, j);
-                        if (bp_ee_ok(A, lo_, hi_)) bp_emit(A, ABD_CONTACT_EE, lo_, hi_);
+                    // a staged box per warp row (in registers), the other side across the lanes
+                    for (int ia = threadIdx.x >> 5; ia < na; ia += blockDim.x >> 5) {
+                        const float4 al = alo[ia], ah = ahi[ia];
+                        const int i = aidx[ia];
+                        for (int ib = threadIdx.x & 31; ib < nbb; ib += 32) {
+                            const int j = bidx[ib];
+                            if (ba == bb && i >= j) continue;
+                            if (!overlap(al, ah, blo[ib], bhi[ib])) continue;
+                            int lo_ = min(i, j), hi_ = max(i, j);
+                            if (bp_ee_ok(A, lo_, hi_)) bp_emit(A, ABD_CONTACT_EE, lo_, hi_);
+                        }
                     }
                     __syncthreads();
                 }
@@ -193,11 +202,14 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp_prims(const int2* __restrict_
                     if (na == 0) continue;
                     for (int t0 = A.tbeg[tb]; t0 < A.tbeg[tb+1]; t0 += BP_CHUNK) {
                         int nt = stage(t0, min(t0 + BP_CHUNK, A.tbeg[tb+1]), rlo, rhi, tbox, bidx, blo, bhi, &sb);
-                        for (long t = threadIdx.x; t < (long)na * nt; t += blockDim.x) {
-                            int ia = (int)(t / nt), ib = (int)(t % nt);
-                            if (!overlap(alo[ia], ahi[ia], blo[ib], bhi[ib])) continue;
-                            int pv = aidx[ia], tr = bidx[ib];
-                            if (bp_pt_ok(A, pv, tr)) bp_emit(A, ABD_CONTACT_PT, pv, tr);
+                        for (int ia = threadIdx.x >> 5; ia < na; ia += blockDim.x >> 5) {
+                            const float4 al = alo[ia], ah = ahi[ia];
+                            const int pv = aidx[ia];
+                            for (int ib = threadIdx.x & 31; ib < nt; ib += 32) {
+                                if (!overlap(al, ah, blo[ib], bhi[ib])) continue;
+                                const int tr = bidx[ib];
+                                if (bp_pt_ok(A, pv, tr)) bp_emit(A, ABD_CONTACT_PT, pv, tr);
+                            }
                         }
                         __syncthreads();
                     }
@@ -221,6 +233,7 @@ __global__ void k_bp_decode(int n, const unsigned long long* __restrict__ keys, 
 
 struct BpScratch {
     float4* blo = nullptr; float4* bhi = nullptr;
+    float4* vlo = nullptr; float4* vhi = nullptr;   // per-vertex boxes of the latest build
     int2* bpairs = nullptr; int bp_cap = 0;
     unsigned long long* keys = nullptr; unsigned long long* keys_s = nullptr; int key_cap = 0;
     int* cnt = nullptr;                     // [0] body pairs, [1] hits, [2] n_ee
@@ -231,7 +244,7 @@ static BpScratch* bps(Engine* E) { return reinterpret_cast<BpScratch*>(E->bp_sta
 void eng_bp_free(Engine* E) {
     BpScratch* S = bps(E);
     if (!S) return;
-    void* ps[] = {S->blo, S->bhi, S->bpairs, S->keys, S->keys_s, S->cnt, S->tmp};
+    void* ps[] = {S->blo, S->bhi, S->vlo, S->vhi, S->bpairs, S->keys, S->keys_s, S->cnt, S->tmp};
     for (void* p : ps) if (p) cudaFree(p);
     delete S;
     E->bp_state = nullptr;
@@ -242,6 +255,8 @@ static int bp_reserve(Engine* E, int bp_need, int key_need) {
     if (!S) {
         S = new BpScratch(); E->bp_state = S;
         if (cudaMalloc(&S->blo, sizeof(float4) * E->nb) != cudaSuccess || cudaMalloc(&S->bhi, sizeof(float4) * E->nb) != cudaSuccess ||
+            cudaMalloc(&S->vlo, sizeof(float4) * std::max(E->nv, 1)) != cudaSuccess ||
+            cudaMalloc(&S->vhi, sizeof(float4) * std::max(E->nv, 1)) != cudaSuccess ||
             cudaMalloc(&S->cnt, sizeof(int) * 4) != cudaSuccess)
             return E->fail(ABD_ERR_CUDA, "cudaMalloc body boxes");
         cudaFuncSetAttribute(k_bp_prims, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -284,11 +299,12 @@ static int bp_build(Engine* E, const double* p, double lim, double filt, int mod
     float pad = (float)(0.5 * lim);
     for (int attempt = 0; attempt < 8; attempt++) {
         CUDA_TRY(cudaMemsetAsync(S->cnt, 0, sizeof(int) * 4, s));
-        k_body_boxes<<<grid_for(32L * E->nb), 256, 0, s>>>(E->nb, E->bd_vbeg, E->x, p, pad, S->blo, S->bhi);
+        k_body_boxes<<<grid_for(32L * E->nb), 256, 0, s>>>(E->nb, E->bd_vbeg, E->x, p, pad, S->blo, S->bhi, S->vlo, S->vhi);
         k_body_pairs<<<grid_for(32L * E->nb), 256, 0, s>>>(E->nb, E->bscene, E->sc_body_begin, S->blo, S->bhi,
                                                             P.self_contact, S->bpairs, S->bp_cap, S->cnt);
         BpArgs A;
         A.G = eng_geo(E); A.p = p; A.pmag = E->pmag; A.ebeg = E->bd_ebeg; A.tbeg = E->bd_tbeg; A.vbeg = E->bd_vbeg;
+        A.vlo = S->vlo; A.vhi = S->vhi;
         A.blo = S->blo; A.bhi = S->bhi; A.pad = pad; A.lim = lim; A.filt = filt; A.mode = mode; A.f32 = P.ee_f32;
         A.self_contact = P.self_contact; A.do_ee = P.contact_ee && E->ne > 0; A.do_pt = P.contact_pt && E->nt > 0;
         A.out = S->keys; A.cap = S->key_cap; A.count = S->cnt + 1;
