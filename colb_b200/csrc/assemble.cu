@@ -282,7 +282,7 @@ DV void warp_distance_derivs(ContactSmem& C, const Geo& G) {
 }
 
 template <class T, int CAW>
-__global__ void __launch_bounds__(32 * CAW) k_contact_assemble(const Counters* cnt, const int4* __restrict__ cst,
+__global__ void __launch_bounds__(32 * CAW, 1) k_contact_assemble(const Counters* cnt, const int4* __restrict__ cst,
                                    const int* __restrict__ ctype, const double* __restrict__ cxb, Geo G, int barrier,
                                    double dhat, double sc, int hess_mode, const int* __restrict__ row_ptr,
                                    const int* __restrict__ bcol, T* vals, double* grad) {
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(32 * CAW) k_contact_assemble(const Counters* c
         const double B1 = C.B1, B2 = C.B2;
         double* A = C.E.A;
         if (hess_mode == ABD_HESS_REFERENCE) {
-            if (C.type == T_EE) warp_psd_project(C.E, 12);               // abd.py:247
+            if (C.type == T_EE) team_psd_project_fast<32>(C.E, 12);      // abd.py:247
             for (int e = lane; e < m * m; e += 32) {
                 int i = e / m, j = e % m;
                 double h = (C.type == T_PP) ? 0.0 : B1 * A[i*12+j];       // abd.py:381-382
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(32 * CAW) k_contact_assemble(const Counters* c
                 A[i*12+j] = B1 * A[i*12+j] + B2 * C.g[i] * C.g[j];
             }
             __syncwarp();
-            warp_psd_project(C.E, m);
+            team_psd_project_fast<32>(C.E, m);
             for (int e = lane; e < m * m; e += 32) { int i = e / m, j = e % m; A[i*12+j] *= sc; }
             __syncwarp();
         }
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(32 * CAW) k_contact_assemble(const Counters* c
 // One block of NT threads per active contact: the same work as
 // k_contact_assemble, with the PSD projection spread over the whole block.
 template <class T, int NT>
-__global__ void __launch_bounds__(NT) k_contact_assemble_team(const Counters* cnt, const int4* __restrict__ cst,
+__global__ void __launch_bounds__(NT, 1) k_contact_assemble_team(const Counters* cnt, const int4* __restrict__ cst,
                                    const int* __restrict__ ctype, const double* __restrict__ cxb, Geo G, int barrier,
                                    double dhat, double sc, int hess_mode, const int* __restrict__ row_ptr,
                                    const int* __restrict__ bcol, T* vals, double* grad) {
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(NT) k_contact_assemble_team(const Counters* cn
         const double B1 = C.B1, B2 = C.B2;
         double* A = C.E.A;
         if (hess_mode == ABD_HESS_REFERENCE) {
-            if (C.type == T_EE) team_psd_project<NT>(C.E, 12);               // abd.py:247
+            if (C.type == T_EE) team_psd_project_fast<NT>(C.E, 12);          // abd.py:247
             for (int e = tid; e < m * m; e += NT) {
                 int i = e / m, j = e % m;
                 double h = (C.type == T_PP) ? 0.0 : B1 * A[i*12+j];       // abd.py:381-382
@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(NT) k_contact_assemble_team(const Counters* cn
                 A[i*12+j] = B1 * A[i*12+j] + B2 * C.g[i] * C.g[j];
             }
             __syncthreads();
-            team_psd_project<NT>(C.E, m);
+            team_psd_project_fast<NT>(C.E, m);
             for (int e = tid; e < m * m; e += NT) { int i = e / m, j = e % m; A[i*12+j] *= sc; }
             __syncthreads();
         }

@@ -342,19 +342,6 @@ constexpr int band_smem_doubles() {
 inline int band_split_point(int n, int wb) { return n >= 2 * wb + 12 ? (n - wb) / 2 : -1; }
 
 
-// 1/sqrt(d): the single-precision estimate r0 (relative error below 2^-22)
-// refined by one third-order Householder step.  With e = 1 - d r0^2,
-// 1/sqrt(d) = r0 (1 - e)^(-1/2) = r0 (1 + e/2 + 3 e^2/8 + O(e^3)): the
-// truncation is below 2^-66, so the result is good to a few ulps after four
-// dependent FP64 operations.  Outside the single-precision range the
-// double-precision rsqrt is used.
-DV double rsqrt_nr(double d) {
-    if (!(d > 1e-30 && d < 1e30)) return rsqrt(d);
-    const double r0 = (double)rsqrtf((float)d);
-    const double e = fma(-d * r0, r0, 1.0);
-    return fma(r0 * e, fma(0.375, e, 0.5), r0);
-}
-
 // Band blocks of every band component, contiguous and in FP64: A(i, i - d)
 // of position i (component order), d = 0..BAND_MAX, row-major, at
 // (loff + i BAND_W + d); blocks outside the band or absent are zero.  One
@@ -401,7 +388,7 @@ DV void band_chol_inverse_rows(double (&a)[12], int* status) {
         if (lane == j) {
             double d = a[j];
             if (!(d > 0.0)) { atomicOr(status, 2); d = fabs(d) + 1e-30; }
-            rown = rsqrt_nr(d);
+            rown = rsqrt(d);        // the double-precision rsqrt: ~76 cycles of latency on sm_100
             s = rown * rown;
         }
         if (j < 11) {

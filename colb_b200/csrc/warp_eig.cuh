@@ -170,3 +170,163 @@ DV void team_psd_project(WarpEigSmem& S, int n) {
 
 DV bool warp_is_pd(WarpEigSmem& S, int n) { return team_is_pd<32>(S, n); }
 DV void warp_psd_project(WarpEigSmem& S, int n) { team_psd_project<32>(S, n); }
+
+// ---------------------------------------------------------------------------
+// Register-resident projection by one warp for n = N (6, 9 or 12).  Lane x
+// holds row x of A and row x of V in registers (M = N rounded up to even;
+// an odd N gets a zero row and column, which no rotation touches).  Every
+// round rotates the fixed pairs (0, 1), (2, 3), ... and then moves the
+// indices one step of the round-robin "circle": index 0 stays, the others
+// advance along 2 -> 4 -> ... -> M-2 -> M-1 -> M-3 -> ... -> 1 -> 2, the
+// same permutation in every round, so M - 1 rounds pair every two indices
+// once and bring them back to their places (one sweep).  The pairing and the
+// permutation being the same in every round, every register index is a
+// constant without unrolling the rounds: the column rotations and the column
+// permutation are moves within a lane, the row rotation is a shuffle with
+// lane x ^ 1 and the row permutation one more shuffle, and the whole round
+// stays a short loop body that the instruction cache holds.  The skip
+// thresholds, the annihilated entry, the stopping rule, the
+// positive-definite early exit and the reconstruction V max(L, 0) V^T are
+// those of team_psd_project; the rotation annihilates a_pq as there, with
+// its tangent t = sgn(d) e / (|d| + sqrt(d^2 + e^2)) (d = a_qq - a_pp,
+// e = 2 a_pq) taken through three double-precision reciprocal square roots.
+template <int N>
+DV bool warp_rows_pd(const double (&a)[N]) {
+    const int lane = threadIdx.x & 31;
+    double l[N];
+#pragma unroll
+    for (int c = 0; c < N; c++) l[c] = a[c];
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const double d = __shfl_sync(0xffffffffu, l[k], k);     // pivot, the same in every lane
+        if (!(d > 0.0)) return false;
+        const double sd = sqrt(d);
+        const double lik = l[k] / sd;                           // L[lane][k] for lanes > k
+        if (lane > k) l[k] = lik;
+#pragma unroll
+        for (int j = k + 1; j < N; j++) {
+            const double ljk = __shfl_sync(0xffffffffu, lik, j);
+            if (lane > k && j <= lane) l[j] -= lik * ljk;
+        }
+    }
+    return true;
+}
+
+// index whose entry moves to position y in one step of the circle (M even)
+HD constexpr int circle_from(int M, int y) {
+    return y == 0 ? 0 : y == 2 ? 1 : y == M - 1 ? M - 2 : (y & 1) ? y + 2 : y - 2;
+}
+
+template <int N>
+DV void warp_psd_project_rows(WarpEigSmem& S) {
+    constexpr int M = (N & 1) ? N + 1 : N;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    double a[M], v[M];
+#pragma unroll
+    for (int c = 0; c < M; c++) {
+        a[c] = (lane < N && c < N) ? S.A[lane * 12 + c] : 0.0;
+        v[c] = (c == lane) ? 1.0 : 0.0;
+    }
+    double fro = 0.0;
+#pragma unroll
+    for (int c = 0; c < M; c++) fro += a[c] * a[c];
+    for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(full, fro, o);
+    if (fro == 0.0) return;
+    {
+        double an[N];
+#pragma unroll
+        for (int c = 0; c < N; c++) an[c] = a[c];
+        if (warp_rows_pd<N>(an)) return;
+    }
+    const double floor2 = 1e-28 * fro;          // (1e-14 of the Frobenius norm)^2
+    const int partner = lane < M ? (lane ^ 1) : lane;
+    const int from = lane < M ? circle_from(M, lane) : lane;
+    for (int sweep = 0; sweep < 50; sweep++) {
+        bool rotated = false;
+#pragma unroll 1
+        for (int r = 0; r < M - 1; r++) {
+            double aii = 0.0, aip = 0.0;
+#pragma unroll
+            for (int c = 0; c < M; c++) { if (c == lane) aii = a[c]; if (c == partner) aip = a[c]; }
+            const double aqq = __shfl_sync(full, aii, partner);
+            // the even lane of a pair computes its rotation
+            double cs = 1.0, sn = 0.0;
+            if (!(lane & 1) && lane < M && aip * aip > fmax(1e-30 * fabs(aii * aqq), floor2)) {
+                const double d = aqq - aii, e = 2.0 * aip;
+                const double h2 = fma(d, d, e * e);
+                const double q = fabs(d) + h2 * rsqrt(h2);
+                const double t = (d >= 0.0 ? e : -e) * rsqrt(q * q);
+                cs = rsqrt(fma(t, t, 1.0)); sn = t * cs;
+            }
+            rotated |= sn != 0.0;
+            // A R and V R: column 2k -> c col_2k - s col_2k+1, column 2k+1 -> s col_2k + c col_2k+1
+#pragma unroll
+            for (int k = 0; k < M / 2; k++) {
+                const double ck = __shfl_sync(full, cs, 2 * k), sk = __shfl_sync(full, sn, 2 * k);
+                const double ap = a[2 * k], aq = a[2 * k + 1], vp = v[2 * k], vq = v[2 * k + 1];
+                a[2 * k] = ck * ap - sk * aq; a[2 * k + 1] = sk * ap + ck * aq;
+                v[2 * k] = ck * vp - sk * vq; v[2 * k + 1] = sk * vp + ck * vq;
+            }
+            // R^T (A R): the even row of a pair -> c row_p - s row_q, the odd one -> s row_p + c row_q
+            const double cm = __shfl_sync(full, cs, lane & ~1), sm = __shfl_sync(full, sn, lane & ~1);
+            const bool even = !(lane & 1);
+#pragma unroll
+            for (int c = 0; c < M; c++) {
+                const double o = __shfl_sync(full, a[c], partner);
+                a[c] = even ? cm * a[c] - sm * o : sm * o + cm * a[c];
+            }
+            // the entry the rotation annihilates is zero, not rounding residue
+            if (sm != 0.0) {
+#pragma unroll
+                for (int c = 0; c < M; c++) if (c == partner) a[c] = 0.0;
+            }
+            // one step of the circle: rows by shuffle, columns (of A and V) by moves
+#pragma unroll
+            for (int c = 0; c < M; c++) a[c] = __shfl_sync(full, a[c], from);
+            double na[M], nv[M];
+#pragma unroll
+            for (int y = 0; y < M; y++) { na[y] = a[circle_from(M, y)]; nv[y] = v[circle_from(M, y)]; }
+#pragma unroll
+            for (int y = 0; y < M; y++) { a[y] = na[y]; v[y] = nv[y]; }
+        }
+        if (!__any_sync(full, rotated)) break;
+    }
+    // H = V max(L, 0) V^T: rows of V and the clamped eigenvalues through shared memory
+    double lam = 0.0;
+#pragma unroll
+    for (int c = 0; c < M; c++) if (c == lane) lam = a[c];
+    if (lane < M) {
+#pragma unroll
+        for (int c = 0; c < M; c++) S.V[lane * 12 + c] = v[c];
+        S.T[lane] = lam > 0 ? lam : 0.0;
+    }
+    __syncwarp();
+    if (lane < N) {
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < M; k++) acc += v[k] * S.T[k] * S.V[j * 12 + k];
+            S.A[lane * 12 + j] = acc;
+        }
+    }
+    __syncwarp();
+}
+
+// All NT threads of a team call it: for n = 6, 9 or 12 the team's first warp
+// projects in registers while the others wait; other sizes take the
+// shared-memory team version.
+template <int NT>
+DV void team_psd_project_fast(WarpEigSmem& S, int n) {
+    if (n == 12 || n == 9 || n == 6) {
+        if ((int)(threadIdx.x % NT) < 32) {
+            if (n == 12) warp_psd_project_rows<12>(S);
+            else if (n == 9) warp_psd_project_rows<9>(S);
+            else warp_psd_project_rows<6>(S);
+        }
+        team_sync<NT>();
+    } else {
+        team_psd_project<NT>(S, n);
+    }
+}

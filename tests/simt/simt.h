@@ -5,10 +5,12 @@
 // dynamic shared memory is one host buffer.  The blocks of a cluster run
 // at the same time (a cluster barrier is a std::barrier over all of their
 // threads, split into arrive and wait); clusters run one after the other.
-// It covers what the direct solver's band kernel uses: its cp.async helpers
-// are plain copies here, so the emulation checks indexing and barriers, not
-// the timing of asynchronous copies; its named barrier 1 is a std::barrier
-// over the whole block that producers arrive at without waiting.  A kernel
+// It covers what the direct solver's band kernel and the warp-level PSD
+// projection of the contact Hessians use.  The band kernel's cp.async
+// helpers are plain copies here, so the emulation checks indexing and
+// barriers, not the timing of asynchronous copies; its named barrier 1 is a
+// std::barrier over the whole block that producers arrive at without
+// waiting; warp votes and shuffles go through the per-warp array.  A kernel
 // that needs anything else (tensor cores, atomics on shared memory,
 // distributed shared memory) does not compile against it.
 #pragma once
@@ -63,6 +65,16 @@ inline double __shfl_sync(unsigned, double v, int src) {
     double r = g_blk->xd[w][src & 31];
     g_blk->warps[w]->arrive_and_wait();
     return r;
+}
+inline double __shfl_xor_sync(unsigned m, double v, int o) { return __shfl_sync(m, v, (int)(threadIdx.x % 32) ^ o); }
+inline bool __any_sync(unsigned, bool pred) {
+    int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    g_blk->xd[w][l] = pred ? 1.0 : 0.0;
+    g_blk->warps[w]->arrive_and_wait();
+    bool any = false;
+    for (int i = 0; i < 32; i++) any = any || g_blk->xd[w][i] != 0.0;
+    g_blk->warps[w]->arrive_and_wait();
+    return any;
 }
 inline float __shfl_sync(unsigned m, float v, int src) { return (float)__shfl_sync(m, (double)v, src); }
 inline int __shfl_sync(unsigned m, int v, int src) { return (int)__shfl_sync(m, (double)v, src); }
