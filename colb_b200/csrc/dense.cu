@@ -327,7 +327,6 @@ constexpr int BAND_THREADS = 256;
 constexpr int BAND_BLK = 146;
 constexpr int BAND_CREC = BAND_W * 144 + 12;   // backward record: factor column blocks, then y_k
 constexpr int BAND_ORD_MAX = 1024;     // bodies of a band component (order kept in shared memory)
-constexpr int BAND_PREFER_MAX = 64;    // above this many bodies cuSOLVER is preferred while it has room
 // dynamic shared memory of k_band_solve in doubles: window, staged block
 // rows, inverse diagonal factors, right-hand sides, y_k, solution blocks,
 // staged right-hand sides, backward records, then the body order (ints)
@@ -1018,11 +1017,10 @@ static int dense_solve_t(Engine* E, int* iters, int* fallback) {
         if (sz < 2 || D->done[E->h_bscene[b]]) continue;
         // FP32 roundings of a stiff projected Hessian can make it indefinite
         // (the band Cholesky has no pivoting), so the band path runs in FP64
-        // mode only; a single CTA walks the band sequentially, so cuSOLVER
-        // (all SMs) is faster for a component above BAND_PREFER_MAX bodies
-        // while few such components exist
-        if (D->root[r] == -1 && projected && !E->mixed &&
-            (sz <= BAND_PREFER_MAX || (int)large_n.size() >= MAX_LARGE_COMPONENTS / 2)) {
+        // mode only; there it takes every component of body bandwidth <= 8,
+        // large ones split between the two CTAs of a cluster, and cuSOLVER
+        // only the components of wider bandwidth
+        if (D->root[r] == -1 && projected && !E->mixed) {
             int bw = rcm(r, ord);
             if (bw >= 1 && bw <= BAND_MAX && sz <= BAND_ORD_MAX) {
                 D->root[r] = -10 - ncomp_band++;          // marks a band component
