@@ -24,10 +24,16 @@ DV int stencil_np(int type) { return type == T_PP ? 2 : (type == T_PE ? 3 : (typ
 DV int other_vertex(int type, int4 s) { return type == T_EE ? s.z : (type == T_PG ? s.x : s.y); }
 
 // ---------------------------------------------------------- prepare + keys
+// Contacts [0, n_total) (the device count); with nkey_pairs > n_total the key
+// pairs of the slots up to nkey_pairs are sentinels (~0), so a sort sized
+// before the count is known sees only real keys and sentinels.
 __global__ void k_contact_prepare(const Counters* cnt, const int4* __restrict__ contacts, Geo G, int f32, double dhat,
                                   int nb, int4* cst, int* ctype, double* cxb, int2* cbody,
-                                  unsigned long long* keys, int* n_active) {
+                                  unsigned long long* keys, int* n_active, int nkey_pairs) {
     int n = cnt->n_total;
+    GS_LOOP(c, nkey_pairs) {
+        if (c >= n) { keys[nb + 2*c] = ~0ull; keys[nb + 2*c + 1] = ~0ull; }
+    }
     GS_LOOP(c, n) {
         int4 C = contacts[c];
         int4 stv; int type = -1; double xb = 0;
@@ -601,25 +607,37 @@ static void launch_contact_assemble(Engine* E, int n, Geo G, double sc, T* V) {
     tune_end(E, TK_CONTACT);
 }
 
-int eng_assemble(Engine* E) {
+// Block keys: the diagonal and one pair per active contact, sorted and made
+// unique, and for the direct solver their copy (with the done flags and the
+// counters) to pinned host memory, where its component analysis reads them.
+// Exact mode runs inside the assembly, sized by the contact count of the
+// last sync, and records an event behind the copies (eng_asm_wait).  Ahead
+// mode runs right after the next iterate's detection, before the
+// end-of-iteration sync that then brings the keys back as well: the new
+// count is not on the host yet, so the keys are sized for the current count
+// plus a quarter and 256 (sentinels beyond the device count; a detection
+// that found more contacts than that discards them, eng_keys_ahead_synced),
+// and no event is needed.
+static int asm_keys(Engine* E, bool ahead, long long& bound) {
     cudaStream_t s = E->stream;
     const AbdParams& P = E->P;
     Geo G = eng_geo(E);
-    int nb = E->nb;
+    const int nb = E->nb;
     int rc;
-    // counters were synchronised by the caller after detection
-    int n = E->hcnt->n_total;
-    int nkeys = nb + 2 * n;
+    const int n_now = E->hcnt->n_total;
+    const int n = ahead ? std::min(E->cap, n_now + n_now / 4 + 256) : n_now;
+    if (ahead) E->keys_ahead_n = n;
+    const int nkeys = nb + 2 * n;
     // room for every block before the count is known: the unique keys are
     // at most the nkeys written and at most every scene's dense pattern,
     // plus the sentinel
-    const long long bound = std::min<long long>(nkeys, E->dense_blocks) + 1;
+    bound = std::min<long long>(nkeys, E->dense_blocks) + 1;
     if (bound > E->blk_cap) { if ((rc = eng_grow_blocks(E, (int)bound))) return rc; }
-    int ph = phase_begin(E, PH_ASM_KEYS);
     CUDA_TRY(cudaMemsetAsync(&E->dcnt->n_active, 0, sizeof(int), s));
     k_diag_keys<<<grid_for(nb), 256, 0, s>>>(nb, E->keys);
     k_contact_prepare<<<grid_for(n > 0 ? n : 1, 128), 128, 0, s>>>(E->dcnt, E->contacts, G, P.ee_f32, P.dhat, nb, E->cst,
-                                                                   E->ctype, E->cxb, E->cbody, E->keys, &E->dcnt->n_active);
+                                                                   E->ctype, E->cxb, E->cbody, E->keys, &E->dcnt->n_active,
+                                                                   ahead ? n : 0);
     int bits = 1;
     while (bits < 64 && ((unsigned long long)nb * nb) >> bits) bits++;
     size_t bytes = E->cub_bytes;
@@ -628,10 +646,6 @@ int eng_assemble(Engine* E) {
     int* n_unique = &E->dcnt->nkeys;
     CUDA_TRY(cub::DeviceSelect::Unique(E->cub_tmp, bytes, E->keys_s, E->ukeys, n_unique, nkeys, s));
     E->launches += 4;
-    // the direct solver's component analysis reads the unique keys on the
-    // host: enqueue their copy (the first nkeys >= unique count) with the
-    // counters behind one event; the assembly kernels are queued after it
-    // and run while the host waits for the keys (eng_asm_wait)
     E->keys_host = false;
     const int ls = E->P.linear_solver;
     const bool direct = ls == ABD_SOLVER_AUTO || ls == ABD_SOLVER_DIRECT;
@@ -651,10 +665,53 @@ int eng_assemble(Engine* E) {
         CUDA_TRY(cudaMemcpyAsync(E->h_ukeys, E->ukeys, sizeof(unsigned long long) * nkeys, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaMemcpyAsync(E->h_done, E->sci + SI_DONE * E->ns, sizeof(int) * E->ns, cudaMemcpyDeviceToHost, s));
     }
-    CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaEventRecord(E->ev_asm, s));
-    E->asm_pending = true;
     E->asm_direct = direct;
+    if (!ahead) {
+        CUDA_TRY(cudaMemcpyAsync(E->hcnt, E->dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaEventRecord(E->ev_asm, s));
+        E->asm_pending = true;
+    }
+    return ABD_OK;
+}
+
+// the next iterate's block keys, queued before the end-of-iteration sync
+int eng_assemble_keys_ahead(Engine* E) {
+    long long bound = 0;
+    int ph = phase_begin(E, PH_ASM_KEYS);
+    int rc = asm_keys(E, true, bound);
+    phase_end(E, ph, 0);
+    if (rc) return rc;
+    E->keys_ahead = true;
+    E->keys_ahead_bound = bound;
+    return ABD_OK;
+}
+
+// after the end-of-iteration sync: keys built ahead are on the host unless
+// the detection they came from overflowed (then the assembly rebuilds them)
+void eng_keys_ahead_synced(Engine* E) {
+    if (!E->keys_ahead) return;
+    if (E->hcnt->overflow || E->hcnt->n_total > E->keys_ahead_n) { E->keys_ahead = false; return; }
+    E->keys_host = E->asm_direct;
+    E->nnzb_host = E->hcnt->nkeys;   // may include the sentinel
+}
+
+int eng_assemble(Engine* E) {
+    cudaStream_t s = E->stream;
+    const AbdParams& P = E->P;
+    Geo G = eng_geo(E);
+    int nb = E->nb;
+    int rc;
+    // counters were synchronised by the caller after detection
+    int n = E->hcnt->n_total;
+    long long bound = 0;
+    int ph = phase_begin(E, PH_ASM_KEYS);
+    if (E->keys_ahead) {
+        bound = E->keys_ahead_bound;      // keys, counters and host copies are there already
+        E->keys_ahead = false;
+    } else if ((rc = asm_keys(E, false, bound))) {
+        return rc;
+    }
+    int* n_unique = &E->dcnt->nkeys;
     const long nnzb = bound;     // launch bound; the kernels read the count from the device
     k_block_rows<<<grid_for(nnzb), 256, 0, s>>>(nb, E->ukeys, n_unique, E->row_ptr, E->bcol, E->dcnt);
     phase_end(E, ph, 0);

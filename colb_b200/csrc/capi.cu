@@ -519,6 +519,7 @@ int abd_energy(AbdHandle* h, double* e) {
 }
 
 static int assemble_full(Engine* E) {
+    E->keys_ahead = false;           // block keys are built by this assembly itself
     CUDA_TRY(cudaMemsetAsync(E->sci + SI_DONE * E->ns, 0, sizeof(int) * E->ns, E->stream));
     int rc = detect_full(E);
     if (rc) return rc;

@@ -160,6 +160,8 @@ struct Engine {
     // the assembly's counters and block keys travel to the host behind
     // ev_asm while its kernels keep running; eng_asm_wait collects them
     cudaEvent_t ev_asm = nullptr; bool asm_pending = false; bool asm_direct = false;
+    // block keys of the next iterate built before the end-of-iteration sync
+    bool keys_ahead = false; long long keys_ahead_bound = 0; int keys_ahead_n = 0;
     int* row_ptr = nullptr; int* bcol = nullptr;
     void* vals = nullptr;          // double or float [blk_cap*144]
     void* dinv = nullptr;          // [nb*144]
@@ -302,6 +304,8 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats);
 int eng_intersections(Engine* E, int* count);
 int eng_sync_counters(Engine* E);
 int eng_asm_wait(Engine* E);                           // counters and block keys of the last assembly on the host
+int eng_assemble_keys_ahead(Engine* E);               // the next iterate's block keys, before the iteration's sync
+void eng_keys_ahead_synced(Engine* E);                // after that sync: keys on the host unless the detection overflowed
 int eng_grid_build(Engine* E, Grid& G);
 GridView eng_view(const Grid& G);
 int eng_swept(Engine* E, const double* dq, double sign, const int* done);

@@ -311,6 +311,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             E->has_ws = 0;
         }
         bool detected_ahead = false;      // this iteration's list filter ran before the last sync
+        E->keys_ahead = false;
         for (int it = 0; it < mi; it++) {
             // contact.py:270-279 detection on the current iterate: filter the
             // swept list of the step that led here, or detect from scratch
@@ -406,8 +407,12 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
                 rc = eng_detect_list(E);
                 phase_end(E, ph, detect_bytes(E));
                 if (rc) return rc;
+                // and the next assembly's block keys, so that this sync
+                // brings them to the direct solver too
+                if ((rc = eng_assemble_keys_ahead(E))) return rc;
             }
             if ((rc = eng_sync_counters(E))) return rc;
+            eng_keys_ahead_synced(E);
             detected_ahead = ahead;
             if (graph_ran) {
                 // the graph's line search ended before the bookkeeping ran
@@ -418,6 +423,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             if (E->hcnt->nan_flag) return E->fail(ABD_ERR_NAN, "non-finite gradient norm");
             if (E->hcnt->scenes_done == ns) break;
         }
+        E->keys_ahead = false;           // keys built for an iteration that did not run
         // counters of this step (the last bookkeeping sync brought them back)
         st.du_guard_hits += E->hcnt->du_guard;
         ccd_capped |= E->hcnt->ccd_capped;
