@@ -17,6 +17,7 @@ ABD_ERR_CCD_CAP = -7
 ABD_ERR_NO_DEVICE = -8
 ABD_ERR_NOT_BUILT = -9
 ABD_INJECT_DU_NONFINITE = 1
+ABD_INJECT_SWEPT_FULL = 2
 ABD_CCD_MAX_ITER = 100000
 
 BARRIER_CUBIC, BARRIER_QUADRATIC, BARRIER_LOG = 0, 1, 2

@@ -220,7 +220,7 @@ int abd_create(const AbdParams* params, const AbdSceneDesc* scenes, int32_t n_sc
     if (!(P.dt > 0) || !(P.dhat > 0) || !(P.cand_dist >= P.dhat) || P.newton_max_iter <= 0 || P.lin_max_iter <= 0 ||
         P.barrier < 0 || P.barrier > 2 || P.contact_capacity <= 0 || P.linear_solver < 0 || P.linear_solver > 3 || (P.ccd && !(P.ccd_scale > 0 && P.ccd_scale < 1)) ||
         P.ls_groups < 0 || P.ls_groups > 1 || P.ls_graph < 0 || P.ls_graph > 1 || P.ccd_max_iter < 0 ||
-        (P.test_inject & ~ABD_INJECT_DU_NONFINITE)) {
+        (P.test_inject & ~(ABD_INJECT_DU_NONFINITE | ABD_INJECT_SWEPT_FULL))) {
         g_err = "abd_create: invalid parameters (dt, dhat <= cand_dist, iteration caps, barrier, capacity, ccd_scale, ls_groups, ls_graph)";
         return ABD_ERR_INVALID_ARG;
     }

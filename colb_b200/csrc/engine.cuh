@@ -143,6 +143,10 @@ struct Engine {
 
     // swept candidate list (swept.cu)
     int4* sw = nullptr; int sw_cap = 0; int n_sw = 0, n_sw_ee = 0; bool sw_valid = false;
+    // fraction of the increment the swept list covers (1 unless the full
+    // step's list did not fit); the line search's step length is capped to it
+    double sw_scale = 1.0;
+    bool sw_inject_done = false;   // ABD_INJECT_SWEPT_FULL fired in this step
     int* sw_nee = nullptr;         // device copy of the list's EE count (the list filter reads it)
     // block keys and done flags of the last assembly, copied to pinned host
     // memory in the assembly's own sync for the direct solver's analysis

@@ -22,10 +22,13 @@ __global__ void k_apply(int nb, const double* __restrict__ backup, const double*
         st[ST_STRIDE * b + ST_NXT + (i % 12)] = __fma_rn(-alpha[s], du[i], backup[i]);
     }
 }
-__global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, const double* toi, int ccd, int* stall) {
+// cap: the fraction of the increment the swept list covers (its CCD bound is a
+// fraction of that shorter step)
+__global__ void k_ls_init(int ns, const int* done, int* acc, double* alpha, const double* toi, int ccd, int* stall,
+                          double cap) {
     GS_LOOP(s, ns) {
         acc[s] = done[s];
-        alpha[s] = ccd ? fmin(1.0, toi[s]) : 1.0;
+        alpha[s] = (ccd ? fmin(1.0, toi[s]) : 1.0) * cap;
         if (!done[s]) stall[s] = 0;
     }
 }
@@ -295,7 +298,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             if (P.ccd && (rc = eng_ccd_list(E, scene_units(E), done))) return rc;
             k_ws_to_du<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->ws, E->mass, E->du);
             k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
-            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd, stall);
+            k_ls_init<<<grid_for(ns), 256, 0, s>>>(ns, done, acc, alpha, E->scd + SD_TOI * ns, P.ccd, stall, E->sw_scale);
             E->launches += 3;
             if ((rc = eng_energy_list(E, scene_units(E), SD_E0, done))) return rc;
             for (int trial = 0;; trial++) {
@@ -312,6 +315,7 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
         }
         bool detected_ahead = false;      // this iteration's list filter ran before the last sync
         E->keys_ahead = false;
+        E->sw_inject_done = false;
         for (int it = 0; it < mi; it++) {
             // contact.py:270-279 detection on the current iterate: filter the
             // swept list of the step that led here, or detect from scratch
@@ -366,7 +370,8 @@ int eng_step(Engine* E, int n_steps, AbdStepStats* stats) {
             { int ph = phase_begin(E, PH_ENERGY); rc = eng_energy_list(E, U, SD_E0, udone); phase_end(E, ph, 0); if (rc) return rc; }
             k_backup<<<grid_for(12L * E->nb), 256, 0, s>>>(E->nb, E->st, E->backup);
             E->launches++;
-            k_ls_init<<<grid_for(U.n), 256, 0, s>>>(U.n, udone, uacc, ualpha, U.d + SD_TOI * U.n, P.ccd, ustall);
+            k_ls_init<<<grid_for(U.n), 256, 0, s>>>(U.n, udone, uacc, ualpha, U.d + SD_TOI * U.n, P.ccd, ustall,
+                                                     E->sw_scale);
             E->launches++;
             int ph_tr = phase_begin(E, PH_TRIALS);
             int graph_ran = 0, graph_body = 0;

@@ -187,12 +187,27 @@ int eng_swept(Engine* E, const double* dq, double sign, const int* done) {
     int rc;
     double lim = P.cand_dist * (1.0 + 1e-6) + 1e-7;
     float pad = (float)(0.5 * lim);
+    E->sw_scale = 1.0;
     if (eng_use_bp(E)) {
         if ((rc = eng_transform(E))) return rc;
-        k_vertex_disp2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, E->vbody, E->xbar, dq, sign, E->mass, E->bscene, done,
-                                                        E->pv, E->pmag);
-        E->launches++;
-        return eng_swept_bp(E, lim);
+        // a candidate list that does not fit even after growing (an increment
+        // that sweeps most primitives into reach) is built for a quarter of
+        // the step, then a sixteenth, ...; the line search then caps its step
+        // length at that fraction (k_ls_init), so the list still covers every
+        // position it visits
+        for (double scale = 1.0;; scale *= 0.25) {
+            k_vertex_disp2<<<grid_for(E->nv), 256, 0, s>>>(E->nv, E->vbody, E->xbar, dq, sign * scale, E->mass, E->bscene,
+                                                            done, E->pv, E->pmag);
+            E->launches++;
+            if ((E->P.test_inject & ABD_INJECT_SWEPT_FULL) && !E->sw_inject_done && scale == 1.0) {
+                E->sw_inject_done = true;        // test hook: the full step's list "does not fit"
+                continue;
+            }
+            rc = eng_swept_bp(E, lim);
+            if (rc == ABD_ERR_CONTACT_OVERFLOW && scale > 1e-6) { E->err.clear(); continue; }
+            if (rc == ABD_OK) E->sw_scale = scale;
+            return rc;
+        }
     }
     for (;;) {
         if ((rc = eng_transform(E))) return rc;

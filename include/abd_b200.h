@@ -128,12 +128,16 @@ typedef struct AbdParams {
     int32_t test_inject;    /* host-side failure injection for tests, 0 in production:
                                ABD_INJECT_DU_NONFINITE overwrites the first Newton increment of
                                every step of scene 0 with NaN before the mixed-precision guard
-                               runs (the guard must replace it by the block-Jacobi direction) */
+                               runs (the guard must replace it by the block-Jacobi direction);
+                               ABD_INJECT_SWEPT_FULL makes the first swept candidate list of every
+                               step report that it does not fit (the list must then be built for a
+                               shorter step, and the step length capped to it) */
     int32_t reserved[1];
 } AbdParams;
 
 #define ABD_CCD_MAX_ITER 100000
 #define ABD_INJECT_DU_NONFINITE 1
+#define ABD_INJECT_SWEPT_FULL 2
 
 /* ---- one scene: concatenated affine bodies (geometry.py:22-73) ------- */
 typedef struct AbdSceneDesc {

@@ -16,6 +16,7 @@ import pytest
 from oracle import oracle as O
 from colb_b200 import params as P, scene as S
 from colb_b200._abi import (ABD_ERR_CCD_CAP, ABD_ERR_NAN, ABD_ERR_SOLVER_CAP, ABD_INJECT_DU_NONFINITE,
+                             ABD_INJECT_SWEPT_FULL,
                             BARRIER_QUADRATIC, SOLVER_PCG)
 from colb_b200.engine import AbdError, Engine
 
@@ -102,6 +103,27 @@ def test_mixed_precision_guard_replaces_a_non_finite_increment():
     plain = Engine(P.config_params(dt=1.0 / 240.0, precision=1), sc)
     rc, st = plain.step(1)
     assert st.du_guard_hits == 0
+
+
+def test_swept_list_that_does_not_fit_caps_the_step_length():
+    """A swept candidate list that does not fit even after growing (an
+    increment that sweeps most primitives into reach) is built for a quarter
+    of the increment, then a sixteenth, ..., and the line search caps its step
+    length at that fraction, so the list still covers every position it
+    visits.  The test hook makes the first list of every step "not fit": the
+    steps must still converge, without intersections, to the positions of a
+    run without the hook."""
+    sc = S.config2_chain_net(n=3, pitch=1.5 - 5e-4, seed=2)
+    a = Engine(P.config_params(dt=1.0 / 240.0, test_inject=ABD_INJECT_SWEPT_FULL), sc)
+    b = Engine(P.config_params(dt=1.0 / 240.0), sc)
+    for _ in range(3):
+        ra, sa = a.step(1)
+        rb, sb = b.step(1)
+        assert ra == 0 and rb == 0 and sa.unconverged == 0 and sb.unconverged == 0
+        assert sa.newton_iters >= sb.newton_iters
+        xa, xb = a.vertices(), b.vertices()
+        assert np.abs(xa - xb).max() <= 1e-6 * np.abs(xb).max()
+    assert a.count_intersections() == 0
 
 
 def test_quadratic_barrier_assembly_and_trajectory(chain_scene, chain_pairs):
