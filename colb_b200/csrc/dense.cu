@@ -604,9 +604,15 @@ k_band_solve(int njobs, const int* __restrict__ jobs, const int* __restrict__ cp
                         int r0t = (tile / 3) * 3, c0t = (tile % 3) * 4;
                         const double* Lia = slot(i, k) + r0t * 12;
                         const double* Ljb = slot(j, k) + c0t * 12;
+                        // rows 0, 4 and 8 of a block share a bank (12 doubles per
+                        // row): the lanes of the three column groups walk the 12
+                        // columns rotated by 0, 1 and 2, so the rows they read at
+                        // once lie on different banks
+                        const int rot = c0t >> 2;
                         double acc[3][4] = {};
 #pragma unroll
-                        for (int s = 0; s < 12; s++) {
+                        for (int s0 = 0; s0 < 12; s0++) {
+                            const int s = s0 + rot < 12 ? s0 + rot : s0 + rot - 12;
                             double li[3], lj[4];
 #pragma unroll
                             for (int a2 = 0; a2 < 3; a2++) li[a2] = Lia[a2 * 12 + s];
