@@ -51,7 +51,8 @@ inline thread_local std::optional<std::barrier<>::arrival_token> g_cluster_tok;
 #define HD inline
 using std::min; using std::max;
 // the device rsqrtf is an approximation (2 ulp); this one is off by a relative
-// 2.3e-7 (close to 2^-22) so that refinements of it are tested from a start as coarse
+// 2.3e-7 (close to 2^-22), so that kernel code refining it is tested from a
+// start as coarse (the kernels run here take the double-precision rsqrt)
 inline float rsqrtf(float x) { return (float)((1.0 / std::sqrt((double)x)) * (1.0 + 2.3e-7)); }
 inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 inline void __syncthreads() { g_blk->block->arrive_and_wait(); }
